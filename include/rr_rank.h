@@ -1,0 +1,153 @@
+/* rr_rank.h -- C ABI of the B200 block-Wiedemann rank engine (librr_b200.so).
+ *
+ * Plain C: pointers, sizes and status codes only.  Every entry point returns
+ * an rr_status; on failure rr_last_error() gives a message for the calling
+ * thread.  Handles are thread-compatible (one thread at a time per handle).
+ * Host arrays passed in are copied; the caller keeps ownership.
+ *
+ * Reference call surface replaced (paths in wilthoma/rust_rank):
+ *   src/vectorstream.rs:7-10      trait VectorStream { next, fill_status }
+ *   src/vectorstream.rs:46,225    NormalVectorStream::new / SimdVectorStream2::new
+ *   src/main.rs:88-216            main_loop_s_mt2 (sequence S_t = V^T B^t V)
+ *   src/sigma_basis.rs:9-54       PM_Basis (minimal generator)
+ *   src/sigma_basis.rs:71-152     analyze_pm_basis -> src/blockbmtest.rs:574-599
+ *   src/wdm_files.rs:22-210       load_wdm_file_sym / save_wdm_file_sym
+ *   src/matrices.rs:662-732       CsrMatrix::load_csr_matrix_from_sms
+ */
+#ifndef RR_RANK_H
+#define RR_RANK_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum rr_status {
+  RR_OK = 0,
+  RR_EINVAL = 1,      /* bad argument (sizes, pointers, indices out of range) */
+  RR_EPRIME = 2,      /* modulus not supported (must be a prime 2 < p < 2^31) */
+  RR_ENOMEM = 3,      /* device or host allocation failed / admission refused */
+  RR_ECUDA = 4,       /* CUDA runtime error */
+  RR_ETIMEOUT = 5,    /* a bounded device-side wait gave up */
+  RR_EIO = 6,         /* file could not be read / written / parsed */
+  RR_ESTATE = 7,      /* call not valid in the handle's current state */
+  RR_EUNSUPPORTED = 8 /* valid request outside what this build implements */
+} rr_status;
+
+typedef struct rr_ctx_s rr_ctx;       /* one device + one CUDA stream */
+typedef struct rr_matrix_s rr_matrix; /* a sparse matrix resident on the device */
+typedef struct rr_krylov_s rr_krylov; /* Krylov state of one block of vectors */
+
+const char* rr_status_string(int status);
+/* Message of the last failed call on this thread ("" if none). */
+const char* rr_last_error(void);
+/* Library version string. */
+const char* rr_version(void);
+
+/* ---------------------------------------------------------------- context */
+int rr_ctx_create(int device, rr_ctx** out);
+int rr_ctx_destroy(rr_ctx* ctx);
+/* The cudaStream_t (as void*) all work of this context is queued on. */
+void* rr_ctx_stream(rr_ctx* ctx);
+int rr_ctx_synchronize(rr_ctx* ctx);
+
+/* ---------------------------------------------------------------- checks */
+/* RR_OK when p is a prime with 2 < p < 2^31, the range the engine computes
+ * in exactly (the reference's overflow check, src/matrices.rs:861-870 and
+ * src/main.rs:481-489, rejects most of these primes for its u32 path; this
+ * engine does not accumulate lazily in 32 bits and has no such limit). */
+int rr_prime_check(uint32_t p);
+
+/* ---------------------------------------------------------------- matrix */
+/* Upload an m x n CSR matrix over F_p.  rowptr[m+1] (int64, rowptr[0] = 0,
+ * non-decreasing), col[nnz] in [0, n), val[nnz] in [0, p) -- the reference's
+ * CsrMatrix<u32> after load (src/matrices.rs:53-64, 662-732).  The device
+ * copy is reordered by degree and transposed once here
+ * (src/matrices.rs:734-778).  Requires nnz < 2^32. */
+int rr_matrix_create(rr_ctx* ctx, int64_t m, int64_t n, const int64_t* rowptr, const int32_t* col,
+                     const uint32_t* val, uint32_t p, rr_matrix** out);
+int rr_matrix_destroy(rr_matrix* mat);
+/* src/matrices.rs:842-860 max_nnzs. */
+int rr_matrix_max_nnzs(const rr_matrix* mat, int64_t* max_row_nnz, int64_t* max_col_nnz);
+int rr_matrix_shape(const rr_matrix* mat, int64_t* m, int64_t* n, int64_t* nnz);
+
+/* ---------------------------------------------------------------- Krylov */
+/* Start (or resume) the Krylov sequence of B = D_c A^T D_r A D_c
+ * (src/main.rs:522-526) for a block of b vectors, 1 <= b <= 32.
+ * row_precond[m], col_precond[n]: diagonal preconditioners in [1, p).
+ * curv[b][n] (vector-major, like Vec<Vec<u32>>): the current block w_k
+ * (= V when seq_len == 0).  seq_len: number of sequence terms already
+ * computed (0 for a fresh start; 1 + 2k after k applications of B). */
+int rr_krylov_create(rr_matrix* mat, int32_t b, const uint32_t* row_precond, const uint32_t* col_precond,
+                     const uint32_t* curv, int64_t seq_len, rr_krylov** out);
+int rr_krylov_destroy(rr_krylov* kr);
+
+/* main_loop_s_mt2 (src/main.rs:88-216) fed by VectorStream::next
+ * (src/vectorstream.rs:58-69): extend the sequence up to max_nlen terms
+ * (a fresh start also emits S_0, so it ends at max_nlen + 1 terms; each
+ * application of B adds two terms).  seq is a HOST array
+ * [b(b+1)/2][seq_stride]; entries [current length, new length) are written,
+ * pair ii enumerating (i <= j) row-major as in src/main.rs:113-127.
+ * *new_len receives the new sequence length. */
+int rr_krylov_advance(rr_krylov* kr, int64_t max_nlen, uint32_t* seq, int64_t seq_stride, int64_t* new_len);
+
+/* Device-resident stepping for benchmarks and pipelines: queue n_apps
+ * applications of B (2 terms each) on the context stream without any host
+ * synchronisation.  Terms stay in the handle's device sequence buffer. */
+int rr_krylov_step_device(rr_krylov* kr, int64_t n_apps);
+/* Copy terms [from, to) of the device sequence buffer into the host array
+ * seq[b(b+1)/2][seq_stride] (synchronises the context stream). */
+int rr_krylov_fetch(rr_krylov* kr, int64_t from, int64_t to, uint32_t* seq, int64_t seq_stride);
+/* Current sequence length (terms computed so far, including queued work). */
+int rr_krylov_length(const rr_krylov* kr, int64_t* len);
+/* The current block w_k as curv[b][n] (host, original column order). */
+int rr_krylov_get_curv(rr_krylov* kr, uint32_t* curv);
+/* Algorithmic bytes of one application of B (both SpMMs: CSR read once,
+ * dense blocks read and written once), for bandwidth reporting. */
+int rr_krylov_bytes_per_application(const rr_krylov* kr, double* bytes);
+
+/* ---------------------------------------------------------------- generator */
+/* PM_Basis (src/sigma_basis.rs:9-54): minimal matrix generator of the
+ * symmetric b x b sequence seq[b(b+1)/2][seq_stride] (nlen valid terms).
+ * d is rounded up to a power of two and must be < nlen.  Outputs (host):
+ * M[2b][2b][d+1] and delta[2b], identical to the reference's result computed
+ * exactly mod p.  Requires p - 1 divisible by the NTT length used (true for
+ * p = 2013265921 = 15*2^27+1 up to d = 2^26). */
+int rr_pm_basis(rr_ctx* ctx, const uint32_t* seq, int64_t seq_stride, int32_t b, int64_t nlen, int64_t d,
+                uint32_t p, uint32_t* M, int64_t* delta);
+/* analyze_pm_basis + analyze_min_generators (src/sigma_basis.rs:71-152,
+ * src/blockbmtest.rs:574-599): rank = b*(k-3) + rank(P[k-1]) + rank(P[0]).
+ * M[2b][2b][len].  RR_ESTATE when k < 3 (no estimate). */
+int rr_rank_from_basis(const uint32_t* M, const int64_t* delta, int32_t b, int64_t len, uint32_t p,
+                       int64_t* rank);
+
+/* Whole pipeline (src/main.rs:463-606): sequence length rule of
+ * src/main.rs:497-504 when max_nlen == 0, Krylov sequence, PM-basis with
+ * d = largest power of two <= length, rank readout. */
+int rr_rank(rr_matrix* mat, int32_t b, const uint32_t* row_precond, const uint32_t* col_precond,
+            const uint32_t* V, int64_t max_nlen, int64_t* rank);
+
+/* ---------------------------------------------------------------- files */
+/* .wdm checkpoint (src/wdm_files.rs:10-19): header "m n p Nlen num_v", then
+ * row_precond, col_precond, num_v lines of v, num_v lines of curv and
+ * num_v(num_v+1)/2 lines of sequence terms. */
+int rr_wdm_save(const char* path, int64_t m, int64_t n, uint32_t p, int32_t b, const uint32_t* row_precond,
+                const uint32_t* col_precond, const uint32_t* v, const uint32_t* curv, const uint32_t* seq,
+                int64_t seq_stride, int64_t nlen);
+/* Two-phase load: call with NULL arrays to read the header into m, n, p, b,
+ * nlen; then again with arrays sized row_precond[m], col_precond[n],
+ * v[b][n], curv[b][n], seq[b(b+1)/2][seq_stride >= nlen]. */
+int rr_wdm_load(const char* path, int64_t* m, int64_t* n, uint32_t* p, int32_t* b, int64_t* nlen,
+                uint32_t* row_precond, uint32_t* col_precond, uint32_t* v, uint32_t* curv, uint32_t* seq,
+                int64_t seq_stride);
+/* SMS text matrix (src/matrices.rs:662-732): "m n M" header then 1-based
+ * "i j v" triplets, values reduced mod p.  Two-phase like rr_wdm_load:
+ * rowptr[m+1], col[nnz], val[nnz]. */
+int rr_sms_load(const char* path, uint32_t p, int64_t* m, int64_t* n, int64_t* nnz, int64_t* rowptr,
+                int32_t* col, uint32_t* val);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RR_RANK_H */

@@ -1,0 +1,309 @@
+"""B200 block-Wiedemann rank engine: Python host layer over librr_b200.so.
+
+Mirrors the reference's call surface for the rank path (wilthoma/rust_rank):
+
+* ``CsrMatrix``            -- src/matrices.rs:53-64 (+ load_csr_matrix_from_sms, max_nnzs)
+* ``KrylovStream``         -- src/vectorstream.rs:7-10 (VectorStream: next, fill_status)
+* ``main_loop_s_mt2``      -- src/main.rs:88-216 (sequence S_t = V^T B^t V, checkpointing)
+* ``PM_Basis``             -- src/sigma_basis.rs:9-54
+* ``analyze_pm_basis``     -- src/sigma_basis.rs:71-152 + src/blockbmtest.rs:574-599 (returns the rank)
+* ``save_wdm_file_sym`` / ``load_wdm_file_sym`` -- src/wdm_files.rs
+* ``block_wiedemann_rank`` -- the driver of src/main.rs:463-606
+
+All arithmetic runs in the CUDA library; nothing here computes on the CPU
+beyond argument marshalling.
+"""
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass
+
+import numpy as np
+
+from ._lib import RRError, check, lib, ptr  # noqa: F401
+import ctypes as C
+
+__all__ = ["Context", "CsrMatrix", "DeviceMatrix", "KrylovStream", "main_loop_s_mt2", "PM_Basis",
+           "analyze_pm_basis", "block_wiedemann_rank", "save_wdm_file_sym", "load_wdm_file_sym",
+           "default_max_nlen", "RRError"]
+
+DEFAULT_PRIME = 2013265921
+
+
+class Context:
+    """One CUDA device and the stream all engine work is queued on."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        check(lib().rr_ctx_create(device, C.byref(h)))
+        self.handle = h
+        self.device = device
+
+    @property
+    def stream(self) -> int:
+        return lib().rr_ctx_stream(self.handle) or 0
+
+    def synchronize(self):
+        check(lib().rr_ctx_synchronize(self.handle))
+
+    def close(self):
+        if self.handle:
+            lib().rr_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_DEFAULT_CTX: Context | None = None
+
+
+def default_context() -> Context:
+    global _DEFAULT_CTX
+    if _DEFAULT_CTX is None:
+        _DEFAULT_CTX = Context(0)
+    return _DEFAULT_CTX
+
+
+@dataclass
+class CsrMatrix:
+    """Host CSR matrix over F_p (src/matrices.rs:53-64); values in [0, p)."""
+
+    values: np.ndarray       # uint32
+    col_indices: np.ndarray  # int32
+    row_ptr: np.ndarray      # int64
+    n_rows: int
+    n_cols: int
+
+    @staticmethod
+    def from_arrays(rowptr, col, val, m, n) -> "CsrMatrix":
+        return CsrMatrix(np.ascontiguousarray(val, np.uint32), np.ascontiguousarray(col, np.int32),
+                         np.ascontiguousarray(rowptr, np.int64), int(m), int(n))
+
+    @staticmethod
+    def load_csr_matrix_from_sms(path: str, theprime: int) -> "CsrMatrix":
+        """src/matrices.rs:662-732."""
+        L = lib()
+        m, n, nnz = C.c_int64(), C.c_int64(), C.c_int64()
+        check(L.rr_sms_load(path.encode(), theprime, C.byref(m), C.byref(n), C.byref(nnz), None, None, None))
+        rowptr = np.zeros(m.value + 1, np.int64)
+        col = np.zeros(max(nnz.value, 1), np.int32)
+        val = np.zeros(max(nnz.value, 1), np.uint32)
+        check(L.rr_sms_load(path.encode(), theprime, C.byref(m), C.byref(n), C.byref(nnz), ptr(rowptr), ptr(col),
+                            ptr(val)))
+        return CsrMatrix(val[: nnz.value], col[: nnz.value], rowptr, m.value, n.value)
+
+    def max_nnzs(self):
+        """src/matrices.rs:842-860."""
+        rows = np.diff(self.row_ptr)
+        cols = np.bincount(self.col_indices, minlength=self.n_cols)
+        return int(rows.max(initial=0)), int(cols.max(initial=0))
+
+    def to_device(self, theprime: int, ctx: Context | None = None) -> "DeviceMatrix":
+        return DeviceMatrix(self, theprime, ctx or default_context())
+
+
+class DeviceMatrix:
+    """A CSR matrix resident on the GPU (degree-ordered copy plus its transpose)."""
+
+    def __init__(self, a: CsrMatrix, theprime: int, ctx: Context):
+        self.ctx = ctx
+        self.p = int(theprime)
+        self.n_rows, self.n_cols = a.n_rows, a.n_cols
+        h = C.c_void_p()
+        check(lib().rr_matrix_create(ctx.handle, a.n_rows, a.n_cols, ptr(a.row_ptr), ptr(a.col_indices),
+                                     ptr(a.values), self.p, C.byref(h)))
+        self.handle = h
+
+    def max_nnzs(self):
+        r, c = C.c_int64(), C.c_int64()
+        check(lib().rr_matrix_max_nnzs(self.handle, C.byref(r), C.byref(c)))
+        return r.value, c.value
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().rr_matrix_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class KrylovStream:
+    """VectorStream (src/vectorstream.rs:7-10) for B = D_c A^T D_r A D_c on the GPU.
+
+    ``next()`` returns w_{k+1} = B w_k as ``b`` host vectors, like the
+    reference's worker threads; ``main_loop_s_mt2`` instead keeps the vectors
+    on the device and only brings back the sequence terms.
+    """
+
+    def __init__(self, a: DeviceMatrix, curv, row_precond, col_precond, seq_len: int = 0):
+        curv = np.ascontiguousarray(curv, np.uint32)
+        self.b = curv.shape[0]
+        self.n = a.n_cols
+        self.a = a
+        self.row_precond = np.ascontiguousarray(row_precond, np.uint32)
+        self.col_precond = np.ascontiguousarray(col_precond, np.uint32)
+        h = C.c_void_p()
+        check(lib().rr_krylov_create(a.handle, self.b, ptr(self.row_precond), ptr(self.col_precond), ptr(curv),
+                                     int(seq_len), C.byref(h)))
+        self.handle = h
+
+    def __len__(self) -> int:
+        v = C.c_int64()
+        check(lib().rr_krylov_length(self.handle, C.byref(v)))
+        return v.value
+
+    def next(self):
+        check(lib().rr_krylov_step_device(self.handle, 1))
+        return list(self.get_curv())
+
+    def fill_status(self) -> str:
+        return "device"
+
+    def get_curv(self) -> np.ndarray:
+        out = np.zeros((self.b, self.n), np.uint32)
+        check(lib().rr_krylov_get_curv(self.handle, ptr(out)))
+        return out
+
+    def advance(self, max_nlen: int, seq: np.ndarray) -> int:
+        new_len = C.c_int64()
+        check(lib().rr_krylov_advance(self.handle, int(max_nlen), ptr(seq), seq.shape[1], C.byref(new_len)))
+        return new_len.value
+
+    def step_device(self, n_apps: int):
+        check(lib().rr_krylov_step_device(self.handle, int(n_apps)))
+
+    def fetch(self, lo: int, hi: int, seq: np.ndarray):
+        check(lib().rr_krylov_fetch(self.handle, int(lo), int(hi), ptr(seq), seq.shape[1]))
+
+    def bytes_per_application(self) -> float:
+        v = C.c_double()
+        check(lib().rr_krylov_bytes_per_application(self.handle, C.byref(v)))
+        return v.value
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().rr_krylov_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def default_max_nlen(m: int, n: int, num_v: int) -> int:
+    """Sequence length rule of src/main.rs:497-504."""
+    max_nlen = int(np.floor(np.float32(2.0) * np.float32(min(m, n)) / np.float32(num_v) + np.float32(4.0)))
+    if num_v > 1:
+        max_nlen = 1 << (max_nlen - 1).bit_length()
+    return max_nlen
+
+
+def main_loop_s_mt2(stream: KrylovStream, row_precond, col_precond, curv, v, seq: np.ndarray, seq_len: int,
+                    max_nlen: int, wdm_filename: str | None = None, theprime: int = DEFAULT_PRIME,
+                    save_after: float = 200.0, chunk_terms: int = 1 << 14) -> int:
+    """src/main.rs:88-216.  ``seq`` is [b(b+1)/2][>= max_nlen + 1] and holds
+    ``seq_len`` terms; returns the new length.  The current block is written
+    back into ``curv`` and, every ``save_after`` seconds, saved to the .wdm file."""
+    last_save = time.time()
+    L = seq_len
+    remaining = max(0, (max_nlen - L) // 2)  # applications of B still to run (src/main.rs:109,131)
+    chunk = max(1, chunk_terms // 2)
+    while True:
+        k = min(remaining, chunk)
+        # a fresh start also emits S_0 (src/main.rs:113-128)
+        L = stream.advance(L + 2 * k if L > 0 else 2 * k, seq)
+        remaining -= k
+        done = remaining == 0
+        if wdm_filename and (done or time.time() - last_save > save_after):
+            curv[:] = stream.get_curv()
+            save_wdm_file_sym(wdm_filename, stream.a.n_rows, stream.n, theprime, row_precond, col_precond, v, curv,
+                              seq[:, :L])
+            last_save = time.time()
+        if done:
+            break
+    curv[:] = stream.get_curv()
+    return L
+
+
+def PM_Basis(seq: np.ndarray, d: int, seqprime: int, ctx: Context | None = None):
+    """src/sigma_basis.rs:9-54 -> (M [2b][2b][d+1], delta [2b])."""
+    ctx = ctx or default_context()
+    seq = np.ascontiguousarray(seq, np.uint32)
+    nn, nlen = seq.shape
+    b = int((np.sqrt(8 * nn + 1) - 1) // 2)
+    if b * (b + 1) // 2 != nn:
+        raise ValueError("Sequence length does not match square matrix size")
+    dd = 1
+    while dd < d:
+        dd *= 2
+    M = np.zeros((2 * b, 2 * b, dd + 1), np.uint32)
+    delta = np.zeros(2 * b, np.int64)
+    check(lib().rr_pm_basis(ctx.handle, ptr(seq), nlen, b, nlen, dd, seqprime, ptr(M), ptr(delta)))
+    return M, delta
+
+
+def analyze_pm_basis(basis: np.ndarray, delta: np.ndarray, p: int) -> int:
+    """src/sigma_basis.rs:71-152 -> src/blockbmtest.rs:574-599; returns the estimated rank."""
+    basis = np.ascontiguousarray(basis, np.uint32)
+    delta = np.ascontiguousarray(delta, np.int64)
+    r = C.c_int64()
+    check(lib().rr_rank_from_basis(ptr(basis), ptr(delta), basis.shape[0] // 2, basis.shape[2], p, C.byref(r)))
+    return r.value
+
+
+def block_wiedemann_rank(a: CsrMatrix | DeviceMatrix, num_v: int, theprime: int = DEFAULT_PRIME,
+                         row_precond=None, col_precond=None, v=None, max_nlen: int = 0, seed: int | None = None,
+                         ctx: Context | None = None) -> int:
+    """The rank path of src/main.rs:463-606 in one call (rr_rank)."""
+    from . import synth
+
+    dm = a if isinstance(a, DeviceMatrix) else a.to_device(theprime, ctx)
+    rng_seed = 0 if seed is None else seed
+    if row_precond is None or col_precond is None:
+        row_precond, col_precond = synth.preconditioners(dm.n_rows, dm.n_cols, theprime, rng_seed + 1)
+    if v is None:
+        v = synth.random_vectors(num_v, dm.n_cols, theprime, rng_seed + 2)
+    row_precond = np.ascontiguousarray(row_precond, np.uint32)
+    col_precond = np.ascontiguousarray(col_precond, np.uint32)
+    v = np.ascontiguousarray(v, np.uint32)
+    r = C.c_int64()
+    check(lib().rr_rank(dm.handle, num_v, ptr(row_precond), ptr(col_precond), ptr(v), int(max_nlen), C.byref(r)))
+    return r.value
+
+
+def save_wdm_file_sym(path: str, n_rows: int, n_cols: int, theprime: int, row_precond, col_precond, v, curv, seq):
+    """src/wdm_files.rs:126-210."""
+    v = np.ascontiguousarray(v, np.uint32)
+    curv = np.ascontiguousarray(curv, np.uint32)
+    seq = np.ascontiguousarray(seq, np.uint32)
+    check(lib().rr_wdm_save(path.encode(), n_rows, n_cols, theprime, v.shape[0],
+                            ptr(np.ascontiguousarray(row_precond, np.uint32)),
+                            ptr(np.ascontiguousarray(col_precond, np.uint32)), ptr(v), ptr(curv), ptr(seq),
+                            seq.shape[1], seq.shape[1]))
+
+
+def load_wdm_file_sym(path: str):
+    """src/wdm_files.rs:22-123 -> (p, m, n, num_v, row_precond, col_precond, v, curv, seq)."""
+    L = lib()
+    m, n, nlen = C.c_int64(), C.c_int64(), C.c_int64()
+    p, b = C.c_uint32(), C.c_int32()
+    check(L.rr_wdm_load(path.encode(), C.byref(m), C.byref(n), C.byref(p), C.byref(b), C.byref(nlen), None, None,
+                        None, None, None, 0))
+    rp = np.zeros(m.value, np.uint32)
+    cp = np.zeros(n.value, np.uint32)
+    v = np.zeros((b.value, n.value), np.uint32)
+    cv = np.zeros((b.value, n.value), np.uint32)
+    seq = np.zeros((b.value * (b.value + 1) // 2, max(nlen.value, 1)), np.uint32)
+    check(L.rr_wdm_load(path.encode(), C.byref(m), C.byref(n), C.byref(p), C.byref(b), C.byref(nlen), ptr(rp),
+                        ptr(cp), ptr(v), ptr(cv), ptr(seq), seq.shape[1]))
+    return p.value, m.value, n.value, b.value, rp, cp, v, cv, seq[:, : nlen.value]

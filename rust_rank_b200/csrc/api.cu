@@ -1,0 +1,411 @@
+// api.cu -- the C ABI (include/rr_rank.h): contexts, matrices, Krylov handles,
+// generator and rank entry points.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+
+#include "rr_internal.h"
+
+namespace rr {
+
+static thread_local std::string g_err;
+
+void set_error(const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+}
+
+int fail(int status, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return status;
+}
+
+uint32_t host_powmod(uint32_t a, uint64_t e, uint32_t p) {
+  uint64_t r = 1 % p, b = a % p;
+  while (e) {
+    if (e & 1) r = r * b % p;
+    b = b * b % p;
+    e >>= 1;
+  }
+  return (uint32_t)r;
+}
+
+uint32_t host_invmod(uint32_t a, uint32_t p) { return host_powmod(a, p - 2, p); }
+
+bool is_prime_u32(uint32_t p) {
+  if (p < 2) return false;
+  if (p % 2 == 0) return p == 2;
+  for (uint64_t d = 3; d * d <= p; d += 2)
+    if (p % d == 0) return false;
+  return true;
+}
+
+ModP make_modp(uint32_t p) {
+  ModP M;
+  M.p = p;
+  M.c32 = (uint32_t)((((uint64_t)1) << 32) % p);
+  M.mu = (uint64_t)(~0ull) / p;  // floor((2^64 - 1) / p) == floor(2^64 / p) for odd p
+  return M;
+}
+
+int launch_scatter_block(rr_krylov* kr, const uint32_t* d_V, uint32_t* d_out);
+
+}  // namespace rr
+
+using namespace rr;
+
+extern "C" {
+
+const char* rr_status_string(int s) {
+  switch (s) {
+    case RR_OK: return "ok";
+    case RR_EINVAL: return "invalid argument";
+    case RR_EPRIME: return "unsupported modulus";
+    case RR_ENOMEM: return "out of memory";
+    case RR_ECUDA: return "CUDA error";
+    case RR_ETIMEOUT: return "device wait timed out";
+    case RR_EIO: return "I/O error";
+    case RR_ESTATE: return "invalid state";
+    case RR_EUNSUPPORTED: return "unsupported";
+  }
+  return "unknown status";
+}
+
+const char* rr_last_error(void) { return g_err.c_str(); }
+
+const char* rr_version(void) { return "rr_b200 0.1 (sm_100a)"; }
+
+int rr_prime_check(uint32_t p) {
+  if (p <= 2 || p >= (1u << 31) || !is_prime_u32(p)) return fail(RR_EPRIME, "p = %u must be a prime in (2, 2^31)", p);
+  return RR_OK;
+}
+
+int rr_ctx_create(int device, rr_ctx** out) {
+  if (!out) return fail(RR_EINVAL, "out is NULL");
+  *out = nullptr;
+  int count = 0;
+  RR_CUDA(cudaGetDeviceCount(&count));
+  if (device < 0 || device >= count) return fail(RR_EINVAL, "device %d not present (%d devices)", device, count);
+  RR_CUDA(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  RR_CUDA(cudaGetDeviceProperties(&prop, device));
+  if (prop.major < 10)
+    return fail(RR_EUNSUPPORTED, "device %d is sm_%d%d; this build targets sm_100a", device, prop.major, prop.minor);
+  std::unique_ptr<rr_ctx> c(new rr_ctx);
+  c->device = device;
+  c->num_sms = prop.multiProcessorCount;
+  RR_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  *out = c.release();
+  return RR_OK;
+}
+
+int rr_ctx_destroy(rr_ctx* ctx) {
+  if (!ctx) return RR_OK;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return RR_OK;
+}
+
+void* rr_ctx_stream(rr_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int rr_ctx_synchronize(rr_ctx* ctx) {
+  if (!ctx) return fail(RR_EINVAL, "ctx is NULL");
+  RR_CUDA(cudaSetDevice(ctx->device));
+  RR_CUDA(cudaStreamSynchronize(ctx->stream));
+  return RR_OK;
+}
+
+int rr_matrix_create(rr_ctx* ctx, int64_t m, int64_t n, const int64_t* rowptr, const int32_t* col,
+                     const uint32_t* val, uint32_t p, rr_matrix** out) {
+  if (!ctx || !out || !rowptr) return fail(RR_EINVAL, "NULL argument");
+  *out = nullptr;
+  RR_TRY(rr_prime_check(p));
+  if (m < 1 || n < 1 || m >= (1ll << 31) || n >= (1ll << 31)) return fail(RR_EINVAL, "bad shape %lld x %lld", (long long)m, (long long)n);
+  if (rowptr[0] != 0) return fail(RR_EINVAL, "rowptr[0] must be 0");
+  for (int64_t r = 0; r < m; ++r)
+    if (rowptr[r + 1] < rowptr[r]) return fail(RR_EINVAL, "rowptr decreases at row %lld", (long long)r);
+  const int64_t nnz = rowptr[m];
+  if (nnz >= (1ll << 32) - 1) return fail(RR_EUNSUPPORTED, "nnz = %lld exceeds 2^32 - 2", (long long)nnz);
+  if (nnz > 0 && (!col || !val)) return fail(RR_EINVAL, "NULL col/val");
+  for (int64_t k = 0; k < nnz; ++k) {
+    if (col[k] < 0 || col[k] >= n) return fail(RR_EINVAL, "column index %d out of range at entry %lld", col[k], (long long)k);
+    if (val[k] >= p) return fail(RR_EINVAL, "value %u at entry %lld is not reduced mod p", val[k], (long long)k);
+  }
+  RR_CUDA(cudaSetDevice(ctx->device));
+  std::unique_ptr<rr_matrix> mat(new rr_matrix);
+  mat->ctx = ctx;
+  mat->m = m;
+  mat->n = n;
+  mat->nnz = nnz;
+  mat->p = p;
+  RR_TRY(matrix_build(ctx, m, n, rowptr, col, val, p, mat.get()));
+  *out = mat.release();
+  return RR_OK;
+}
+
+int rr_matrix_destroy(rr_matrix* mat) {
+  if (!mat) return RR_OK;
+  cudaSetDevice(mat->ctx->device);
+  cudaStreamSynchronize(mat->ctx->stream);
+  delete mat;
+  return RR_OK;
+}
+
+int rr_matrix_max_nnzs(const rr_matrix* mat, int64_t* max_row, int64_t* max_col) {
+  if (!mat || !max_row || !max_col) return fail(RR_EINVAL, "NULL argument");
+  *max_row = mat->max_row_nnz;
+  *max_col = mat->max_col_nnz;
+  return RR_OK;
+}
+
+int rr_matrix_shape(const rr_matrix* mat, int64_t* m, int64_t* n, int64_t* nnz) {
+  if (!mat || !m || !n || !nnz) return fail(RR_EINVAL, "NULL argument");
+  *m = mat->m;
+  *n = mat->n;
+  *nnz = mat->nnz;
+  return RR_OK;
+}
+
+// ---------------------------------------------------------------- Krylov
+static int padded_width(int b) { return b <= 4 ? 4 : b <= 8 ? 8 : b <= 16 ? 16 : 32; }
+
+static int ensure_capacity(rr_krylov* kr, int64_t terms) {
+  const int np = kr->b * (kr->b + 1) / 2;
+  if (terms <= kr->cap) return RR_OK;
+  int64_t ncap = std::max<int64_t>(terms, 2 * kr->cap);
+  DevBuf<uint32_t> nb;
+  RR_TRY(nb.alloc((size_t)ncap * np));
+  if (kr->cap > 0)
+    RR_CUDA(cudaMemcpyAsync(nb.ptr, kr->S.ptr, (size_t)kr->cap * np * 4, cudaMemcpyDeviceToDevice, kr->mat->ctx->stream));
+  RR_CUDA(cudaStreamSynchronize(kr->mat->ctx->stream));
+  std::swap(kr->S.ptr, nb.ptr);
+  std::swap(kr->S.n, nb.n);
+  kr->cap = ncap;
+  return RR_OK;
+}
+
+int rr_krylov_create(rr_matrix* mat, int32_t b, const uint32_t* row_precond, const uint32_t* col_precond,
+                     const uint32_t* curv, int64_t seq_len, rr_krylov** out) {
+  if (!mat || !out || !row_precond || !col_precond || !curv) return fail(RR_EINVAL, "NULL argument");
+  *out = nullptr;
+  if (b < 1 || b > 32) return fail(RR_EINVAL, "block width b = %d must be in [1, 32]", b);
+  if (seq_len < 0) return fail(RR_EINVAL, "seq_len < 0");
+  const uint32_t p = mat->p;
+  const int64_t m = mat->m, n = mat->n;
+  for (int64_t i = 0; i < m; ++i)
+    if (row_precond[i] == 0 || row_precond[i] >= p) return fail(RR_EINVAL, "row_precond[%lld] not in [1, p)", (long long)i);
+  for (int64_t i = 0; i < n; ++i)
+    if (col_precond[i] == 0 || col_precond[i] >= p) return fail(RR_EINVAL, "col_precond[%lld] not in [1, p)", (long long)i);
+  for (int64_t i = 0; i < (int64_t)b * n; ++i)
+    if (curv[i] >= p) return fail(RR_EINVAL, "curv entry %lld not reduced mod p", (long long)i);
+  rr_ctx* ctx = mat->ctx;
+  RR_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  std::unique_ptr<rr_krylov> kr(new rr_krylov);
+  kr->mat = mat;
+  kr->b = b;
+  kr->B = padded_width(b);
+  kr->M = make_modp(p);
+  {
+    // four products fit between folds iff (2^32-1)*c32 + 2^32 - 1 + 4 (p-1)^2 < 2^64
+    const unsigned __int128 F = (unsigned __int128)0xffffffffull * kr->M.c32 + 0xffffffffull;
+    const unsigned __int128 q = (unsigned __int128)(p - 1) * (p - 1);
+    kr->fold4 = (F + 4 * q) < ((unsigned __int128)1 << 64);
+  }
+  // preconditioners in device order; D_c^{-1} by one inversion and prefix products
+  std::vector<uint32_t> dr(m), dc(n), dci(n);
+  for (int64_t i = 0; i < m; ++i) dr[i] = row_precond[mat->rowperm[i]];
+  for (int64_t i = 0; i < n; ++i) dc[i] = col_precond[mat->colperm[i]];
+  {
+    std::vector<uint32_t> pre(n + 1);
+    pre[0] = 1;
+    for (int64_t i = 0; i < n; ++i) pre[i + 1] = (uint32_t)((uint64_t)pre[i] * dc[i] % p);
+    uint64_t inv = host_invmod(pre[n], p);
+    for (int64_t i = n - 1; i >= 0; --i) {
+      dci[i] = (uint32_t)(inv * pre[i] % p);
+      inv = inv * dc[i] % p;
+    }
+  }
+  RR_TRY(kr->dr.alloc(m));
+  RR_TRY(kr->dc.alloc(n));
+  RR_TRY(kr->dcinv.alloc(n));
+  RR_CUDA(cudaMemcpyAsync(kr->dr.ptr, dr.data(), m * 4, cudaMemcpyHostToDevice, s));
+  RR_CUDA(cudaMemcpyAsync(kr->dc.ptr, dc.data(), n * 4, cudaMemcpyHostToDevice, s));
+  RR_CUDA(cudaMemcpyAsync(kr->dcinv.ptr, dci.data(), n * 4, cudaMemcpyHostToDevice, s));
+  const int B = kr->B;
+  RR_TRY(kr->X[0].alloc((size_t)n * B));
+  RR_TRY(kr->X[1].alloc((size_t)n * B));
+  RR_TRY(kr->U.alloc((size_t)m * B));
+  const int64_t heavy = std::max<int64_t>(std::max(mat->A.heavy_rows, mat->At.heavy_rows), 1);
+  RR_TRY(kr->heavy_acc.alloc((size_t)heavy * B));
+  RR_CUDA(cudaMemsetAsync(kr->heavy_acc.ptr, 0, kr->heavy_acc.bytes(), s));
+  RR_TRY(kr->gram_acc.alloc(B * (B + 1) / 2));
+  RR_CUDA(cudaMemsetAsync(kr->gram_acc.ptr, 0, kr->gram_acc.bytes(), s));
+  RR_TRY(kr->counter.alloc(4));
+  RR_CUDA(cudaMemsetAsync(kr->counter.ptr, 0, kr->counter.bytes(), s));
+  RR_TRY(krylov_occupancy(kr.get()));
+  kr->base = seq_len;
+  kr->len = seq_len;
+  RR_TRY(ensure_capacity(kr.get(), 64));
+  // upload curv (vector-major), scatter into device order, x = D_c w
+  {
+    DevBuf<uint32_t> v;
+    RR_TRY(v.alloc((size_t)b * n));
+    RR_CUDA(cudaMemcpyAsync(v.ptr, curv, (size_t)b * n * 4, cudaMemcpyHostToDevice, s));
+    RR_TRY(launch_scatter_block(kr.get(), v.ptr, kr->X[1].ptr));
+    kr->cur = 0;
+    // S_0 is computed now into slot 0 and published by the first advance
+    RR_TRY(krylov_launch_init(kr.get(), kr->X[1].ptr, seq_len == 0));
+    RR_CUDA(cudaStreamSynchronize(s));
+  }
+  *out = kr.release();
+  return RR_OK;
+}
+
+int rr_krylov_destroy(rr_krylov* kr) {
+  if (!kr) return RR_OK;
+  cudaSetDevice(kr->mat->ctx->device);
+  cudaStreamSynchronize(kr->mat->ctx->stream);
+  delete kr;
+  return RR_OK;
+}
+
+static int queue_apps(rr_krylov* kr, int64_t n_apps) {
+  if (kr->len == 0) kr->len = 1;  // publish S_0
+  RR_TRY(ensure_capacity(kr, kr->len - kr->base + 2 * n_apps + 1));
+  for (int64_t i = 0; i < n_apps; ++i) RR_TRY(krylov_launch_application(kr));
+  return RR_OK;
+}
+
+int rr_krylov_step_device(rr_krylov* kr, int64_t n_apps) {
+  if (!kr) return fail(RR_EINVAL, "NULL handle");
+  if (n_apps < 0) return fail(RR_EINVAL, "n_apps < 0");
+  RR_CUDA(cudaSetDevice(kr->mat->ctx->device));
+  return queue_apps(kr, n_apps);
+}
+
+int rr_krylov_fetch(rr_krylov* kr, int64_t from, int64_t to, uint32_t* seq, int64_t seq_stride) {
+  if (!kr || (!seq && to > from)) return fail(RR_EINVAL, "NULL argument");
+  if (from < kr->base || to > kr->len || from > to)
+    return fail(RR_EINVAL, "terms [%lld, %lld) not held (held: [%lld, %lld))", (long long)from, (long long)to,
+                (long long)kr->base, (long long)kr->len);
+  if (seq_stride < to) return fail(RR_EINVAL, "seq_stride %lld < %lld", (long long)seq_stride, (long long)to);
+  RR_CUDA(cudaSetDevice(kr->mat->ctx->device));
+  const int np = kr->b * (kr->b + 1) / 2;
+  const int64_t cnt = to - from;
+  if (cnt == 0) return RR_OK;
+  std::vector<uint32_t> tmp((size_t)cnt * np);
+  RR_CUDA(cudaMemcpyAsync(tmp.data(), kr->S.ptr + (size_t)(from - kr->base) * np, tmp.size() * 4,
+                          cudaMemcpyDeviceToHost, kr->mat->ctx->stream));
+  RR_CUDA(cudaStreamSynchronize(kr->mat->ctx->stream));
+  for (int64_t t = 0; t < cnt; ++t)
+    for (int q = 0; q < np; ++q) seq[(size_t)q * seq_stride + from + t] = tmp[(size_t)t * np + q];
+  return RR_OK;
+}
+
+int rr_krylov_advance(rr_krylov* kr, int64_t max_nlen, uint32_t* seq, int64_t seq_stride, int64_t* new_len) {
+  if (!kr || !seq || !new_len) return fail(RR_EINVAL, "NULL argument");
+  RR_CUDA(cudaSetDevice(kr->mat->ctx->device));
+  const int64_t L0 = kr->len;
+  const int64_t to_be_produced = max_nlen - L0;  // src/main.rs:109
+  if (to_be_produced < 0) {
+    *new_len = L0;
+    return RR_OK;
+  }
+  const int64_t final_len = (L0 == 0 ? 1 : L0) + 2 * (to_be_produced / 2);
+  if (seq_stride < final_len) return fail(RR_EINVAL, "seq_stride %lld < %lld terms", (long long)seq_stride, (long long)final_len);
+  RR_TRY(queue_apps(kr, to_be_produced / 2));
+  RR_TRY(rr_krylov_fetch(kr, L0, kr->len, seq, seq_stride));
+  *new_len = kr->len;
+  return RR_OK;
+}
+
+int rr_krylov_length(const rr_krylov* kr, int64_t* len) {
+  if (!kr || !len) return fail(RR_EINVAL, "NULL argument");
+  *len = kr->len;
+  return RR_OK;
+}
+
+int rr_krylov_get_curv(rr_krylov* kr, uint32_t* curv) {
+  if (!kr || !curv) return fail(RR_EINVAL, "NULL argument");
+  RR_CUDA(cudaSetDevice(kr->mat->ctx->device));
+  DevBuf<uint32_t> out;
+  RR_TRY(out.alloc((size_t)kr->b * kr->mat->n));
+  RR_TRY(krylov_launch_get_curv(kr, out.ptr));
+  RR_CUDA(cudaMemcpyAsync(curv, out.ptr, out.bytes(), cudaMemcpyDeviceToHost, kr->mat->ctx->stream));
+  RR_CUDA(cudaStreamSynchronize(kr->mat->ctx->stream));
+  return RR_OK;
+}
+
+int rr_krylov_bytes_per_application(const rr_krylov* kr, double* bytes) {
+  if (!kr || !bytes) return fail(RR_EINVAL, "NULL argument");
+  const rr_matrix* m = kr->mat;
+  const double csr = 2.0 * (8.0 * (double)m->nnz) + 4.0 * ((double)m->m + 1) + 4.0 * ((double)m->n + 1);
+  *bytes = csr + 4.0 * kr->b * 2.0 * ((double)m->m + (double)m->n);
+  return RR_OK;
+}
+
+// ---------------------------------------------------------------- generator
+int rr_pm_basis(rr_ctx* ctx, const uint32_t* seq, int64_t seq_stride, int32_t b, int64_t nlen, int64_t d, uint32_t p,
+                uint32_t* M, int64_t* delta) {
+  if (!ctx || !seq || !M || !delta) return fail(RR_EINVAL, "NULL argument");
+  RR_TRY(rr_prime_check(p));
+  if (b < 1 || b > 32) return fail(RR_EINVAL, "b = %d must be in [1, 32]", b);
+  if (seq_stride < nlen) return fail(RR_EINVAL, "seq_stride < nlen");
+  int64_t dd = 1;
+  while (dd < d) dd *= 2;
+  if (dd >= nlen) return fail(RR_EINVAL, "sequence too short: d = %lld, nlen = %lld", (long long)dd, (long long)nlen);
+  RR_CUDA(cudaSetDevice(ctx->device));
+  return pm_basis_device(ctx, seq, seq_stride, b, nlen, dd, p, M, delta);
+}
+
+int rr_rank_from_basis(const uint32_t* M, const int64_t* delta, int32_t b, int64_t len, uint32_t p, int64_t* rank) {
+  if (!M || !delta || !rank) return fail(RR_EINVAL, "NULL argument");
+  if (b < 1 || len < 1) return fail(RR_EINVAL, "bad sizes");
+  return rank_from_basis_host(M, delta, b, len, p, rank);
+}
+
+int rr_rank(rr_matrix* mat, int32_t b, const uint32_t* row_precond, const uint32_t* col_precond, const uint32_t* V,
+            int64_t max_nlen, int64_t* rank) {
+  if (!mat || !rank) return fail(RR_EINVAL, "NULL argument");
+  if (b < 1 || b > 32) return fail(RR_EINVAL, "b = %d must be in [1, 32]", b);
+  if (max_nlen <= 0) {  // src/main.rs:497-504
+    const float dmin = (float)std::min(mat->m, mat->n);
+    max_nlen = (int64_t)std::floor(2.0f * dmin / (float)b + 4.0f);
+  }
+  if (b > 1) {
+    int64_t q = 1;
+    while (q < max_nlen) q *= 2;
+    max_nlen = q;
+  }
+  rr_krylov* kr = nullptr;
+  RR_TRY(rr_krylov_create(mat, b, row_precond, col_precond, V, 0, &kr));
+  std::unique_ptr<rr_krylov, int (*)(rr_krylov*)> guard(kr, rr_krylov_destroy);
+  const int np = b * (b + 1) / 2;
+  const int64_t stride = max_nlen + 1;
+  std::vector<uint32_t> seq((size_t)np * stride);
+  int64_t L = 0;
+  RR_TRY(rr_krylov_advance(kr, max_nlen, seq.data(), stride, &L));
+  int64_t d = 1;  // src/main.rs:599-603
+  while (d <= L) d *= 2;
+  d /= 2;
+  std::vector<uint32_t> M((size_t)(2 * b) * (2 * b) * (d + 1));
+  std::vector<int64_t> delta(2 * b);
+  RR_TRY(rr_pm_basis(mat->ctx, seq.data(), stride, b, L, d, mat->p, M.data(), delta.data()));
+  return rr_rank_from_basis(M.data(), delta.data(), b, d + 1, mat->p, rank);
+}
+
+}  // extern "C"

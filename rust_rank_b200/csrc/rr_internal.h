@@ -1,0 +1,137 @@
+// rr_internal.h -- host-side internals shared by the engine's translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "rr_modp.cuh"
+#include "rr_rank.h"
+
+namespace rr {
+
+// Thread-local error message behind rr_last_error().
+void set_error(const char* fmt, ...);
+int fail(int status, const char* fmt, ...);
+
+#define RR_CUDA(call)                                                                            \
+  do {                                                                                           \
+    cudaError_t e_ = (call);                                                                     \
+    if (e_ != cudaSuccess)                                                                       \
+      return ::rr::fail(e_ == cudaErrorMemoryAllocation ? RR_ENOMEM : RR_ECUDA, "%s: %s (%s:%d)", \
+                        #call, cudaGetErrorString(e_), __FILE__, __LINE__);                      \
+  } while (0)
+
+#define RR_TRY(expr)          \
+  do {                        \
+    int s_ = (expr);          \
+    if (s_ != RR_OK) return s_; \
+  } while (0)
+
+ModP make_modp(uint32_t p);
+bool is_prime_u32(uint32_t p);
+uint32_t host_powmod(uint32_t a, uint64_t e, uint32_t p);
+uint32_t host_invmod(uint32_t a, uint32_t p);
+
+// Owning device buffer.
+template <class T>
+struct DevBuf {
+  T* ptr = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    n = 0;
+  }
+  int alloc(size_t count) {
+    release();
+    if (count == 0) return RR_OK;
+    cudaError_t e = cudaMalloc((void**)&ptr, count * sizeof(T));
+    if (e != cudaSuccess) {
+      ptr = nullptr;
+      cudaGetLastError();
+      return fail(RR_ENOMEM, "cudaMalloc of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
+    }
+    n = count;
+    return RR_OK;
+  }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+}  // namespace rr
+
+struct rr_ctx_s {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int num_sms = 0;
+};
+
+namespace rr {
+
+// Degree-sorted CSR resident on the device.  Rows [0, heavy_rows) have more
+// than kHeavyDegree entries and are processed by the chunk kernel.
+struct DevCsr {
+  DevBuf<uint32_t> rowptr;  // rows + 1 offsets
+  DevBuf<int32_t> col;
+  DevBuf<uint32_t> val;
+  int64_t rows = 0, cols = 0, nnz = 0;
+  int64_t heavy_rows = 0;
+  int64_t nchunks = 0;
+  DevBuf<uint32_t> chunk_row, chunk_begin, chunk_end;
+};
+
+constexpr int64_t kHeavyDegree = 512;  // rows longer than this are split
+constexpr int64_t kChunkNnz = 1024;    // nonzeros per chunk of a split row
+
+}  // namespace rr
+
+struct rr_matrix_s {
+  rr_ctx* ctx = nullptr;
+  int64_t m = 0, n = 0, nnz = 0;
+  uint32_t p = 0;
+  int64_t max_row_nnz = 0, max_col_nnz = 0;
+  rr::DevCsr A;   // rows of A in degree order, columns renumbered in degree order
+  rr::DevCsr At;  // its transpose
+  std::vector<int32_t> rowperm;  // rowperm[r'] = original row
+  std::vector<int32_t> colperm;  // colperm[c'] = original column
+  rr::DevBuf<int32_t> d_colperm;
+};
+
+struct rr_krylov_s {
+  rr_matrix* mat = nullptr;
+  int b = 0;   // real block width
+  int B = 0;   // padded width (4, 8, 16, 32)
+  rr::ModP M{};
+  int fold4 = 0;  // 1 when four products fit between folds
+  rr::DevBuf<uint32_t> dr, dc, dcinv;  // preconditioners in device order
+  rr::DevBuf<uint32_t> X[2];           // x_k = D_c w_k, n x B interleaved
+  rr::DevBuf<uint32_t> U;              // D_r A x_k, m x B
+  rr::DevBuf<unsigned long long> heavy_acc;
+  rr::DevBuf<unsigned long long> gram_acc;
+  rr::DevBuf<unsigned int> counter;
+  rr::DevBuf<uint32_t> S;  // device sequence, [cap][np]
+  int64_t cap = 0;
+  int64_t base = 0; // first term held in S
+  int64_t len = 0;  // terms queued so far
+  int cur = 0;      // index of the current X
+  int grid_pass = 0, grid_chunk = 0;
+};
+
+namespace rr {
+int krylov_launch_init(rr_krylov* kr, const uint32_t* d_w, bool emit_s0);
+int krylov_launch_application(rr_krylov* kr);
+int krylov_launch_get_curv(rr_krylov* kr, uint32_t* d_out);
+int krylov_occupancy(rr_krylov* kr);
+int matrix_build(rr_ctx* ctx, int64_t m, int64_t n, const int64_t* rowptr, const int32_t* col,
+                 const uint32_t* val, uint32_t p, rr_matrix* mat);
+// PM-basis on the device; M (host) [2b][2b][d+1], delta (host) [2b].
+int pm_basis_device(rr_ctx* ctx, const uint32_t* seq, int64_t seq_stride, int b, int64_t nlen, int64_t d,
+                    uint32_t p, uint32_t* M, int64_t* delta);
+int rank_from_basis_host(const uint32_t* M, const int64_t* delta, int b, int64_t len, uint32_t p, int64_t* rank);
+}  // namespace rr

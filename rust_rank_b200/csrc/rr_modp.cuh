@@ -1,0 +1,53 @@
+// rr_modp.cuh -- exact arithmetic modulo a prime p < 2^31 on sm_100a.
+//
+// Values are kept as uint32 in [0, p).  Dot products and sparse row sums are
+// accumulated lazily in 64 bits: a product of two residues is < p^2 < 2^62,
+// and an accumulator is "folded" (hi * (2^32 mod p) + lo) after every
+// `fold_every` products so that it never wraps.  The final residue comes from
+// a Barrett reduction with mu = floor(2^64 / p) (Barrett, CRYPTO '86).
+#pragma once
+#include <cstdint>
+
+namespace rr {
+
+struct ModP {
+  uint32_t p;      // the prime, p < 2^31
+  uint32_t c32;    // 2^32 mod p
+  uint64_t mu;     // floor(2^64 / p)
+};
+
+#ifdef __CUDACC__
+// Fold a 64-bit accumulator: result == x (mod p) and result < 2^32 * c32 + 2^32.
+__device__ __forceinline__ uint64_t fold(uint64_t x, const ModP& M) {
+  return (uint64_t)(uint32_t)(x >> 32) * M.c32 + (uint32_t)x;
+}
+
+// Exact x mod p for any 64-bit x.  q = floor(x*mu / 2^64) is at most 2 below
+// floor(x/p), so r = x - q*p < 3p and two conditional subtractions finish.
+__device__ __forceinline__ uint32_t reduce(uint64_t x, const ModP& M) {
+  const uint64_t q = __umul64hi(x, M.mu);
+  uint64_t r = x - q * (uint64_t)M.p;
+  if (r >= M.p) r -= M.p;
+  if (r >= M.p) r -= M.p;
+  return (uint32_t)r;
+}
+
+__device__ __forceinline__ uint32_t mulmod(uint32_t a, uint32_t b, const ModP& M) {
+  return reduce((uint64_t)a * b, M);
+}
+
+__device__ __forceinline__ uint32_t addmod(uint32_t a, uint32_t b, uint32_t p) {
+  const uint32_t s = a + b;  // a, b < 2^31 so no wrap
+  return s >= p ? s - p : s;
+}
+
+__device__ __forceinline__ uint32_t submod(uint32_t a, uint32_t b, uint32_t p) {
+  return a >= b ? a - b : a + p - b;
+}
+
+__device__ __forceinline__ uint64_t mad_wide(uint32_t a, uint32_t b, uint64_t c) {
+  return (uint64_t)a * b + c;
+}
+#endif  // __CUDACC__
+
+}  // namespace rr

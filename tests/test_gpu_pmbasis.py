@@ -1,0 +1,70 @@
+"""Parity of the CUDA PM-basis and of the whole rank pipeline with the oracle
+and with the reference's own golden outputs (bit-exact)."""
+import numpy as np
+import pytest
+
+import oracle
+import rust_rank_b200 as rr
+from rust_rank_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+P = 2013265921
+
+
+def test_golden_reference_pm_basis_small_prime(ctx, golden):
+    z = golden("pm_basis_ref.npz")
+    for i in range(int(z["count"])):
+        b, d, rank = (int(x) for x in z[f"c{i}_meta"])
+        M, delta = rr.PM_Basis(z[f"c{i}_seq"], d, 3323, ctx)
+        assert np.array_equal(M, z[f"c{i}_M"]), f"case {i} b={b} d={d}"
+        assert np.array_equal(delta, z[f"c{i}_delta"]), f"case {i}"
+
+
+@pytest.mark.parametrize("b,d", [(1, 1), (1, 64), (2, 2), (2, 256), (3, 40), (4, 8), (4, 128), (8, 32), (8, 64),
+                                 (8, 1024), (16, 16), (16, 33), (16, 256), (32, 8), (32, 64)])
+def test_random_sequences_vs_oracle(ctx, b, d):
+    rng = np.random.default_rng(b * 1000 + d)
+    dd = 1 << (d - 1).bit_length()
+    seq = rng.integers(0, P, size=(b * (b + 1) // 2, dd + 2)).astype(np.uint32)
+    M, delta = rr.PM_Basis(seq, d, P, ctx)
+    Mo, do = oracle.pm_basis(seq, b, d, P)
+    assert np.array_equal(M, Mo.astype(np.uint32))
+    assert np.array_equal(delta, do)
+
+
+def test_structured_sequence_with_dependent_rows(ctx):
+    """A low-rank sequence exercises rows without pivots in every leaf."""
+    b, d = 8, 128
+    rng = np.random.default_rng(3)
+    rowptr, col, val, m, n = synth.incidence(40, 30, seed=2)  # rank <= 30, tiny
+    dr, dc = synth.preconditioners(m, n, P, 1)
+    V = synth.random_vectors(b, n, P, 2)
+    seq, L, _ = oracle.krylov(rowptr, col, val, m, n, P, dr, dc, V, 0, 2 * d)
+    M, delta = rr.PM_Basis(seq, d, P, ctx)
+    Mo, do = oracle.pm_basis(seq, b, d, P)
+    assert np.array_equal(M, Mo.astype(np.uint32)) and np.array_equal(delta, do)
+    assert rr.analyze_pm_basis(M, delta, P) == oracle.rank_from_basis(Mo, do, P)
+    del rng
+
+
+@pytest.mark.parametrize("p", [3323, 27644437, P])
+@pytest.mark.parametrize("b", [1, 2, 4, 8])
+def test_rank_of_matrix_txt(ctx, matrix_txt, p, b):
+    rowptr, col, sval, m, n = matrix_txt
+    val = (sval.astype(np.int64) % p).astype(np.uint32)
+    a = rr.CsrMatrix.from_arrays(rowptr, col, val, m, n)
+    assert rr.block_wiedemann_rank(a, b, p, seed=b, ctx=ctx) == 104
+
+
+@pytest.mark.parametrize("b", [4, 8, 16])
+def test_rank_known_by_construction(ctx, b):
+    rowptr, col, val, m, n = synth.plain_single(n=1200, k=6, dep_rows=40, seed=b)
+    dense = oracle.dense_rank_csr(rowptr, col, val, m, n, P)
+    assert dense <= 1160
+    a = rr.CsrMatrix.from_arrays(rowptr, col, val, m, n)
+    assert rr.block_wiedemann_rank(a, b, P, seed=7, ctx=ctx) == dense
+    rp, cp = synth.preconditioners(m, n, P, 8)
+    V = synth.random_vectors(b, n, P, 9)
+    r_orc, _, _, _ = oracle.rank_pipeline(rowptr, col, val, m, n, P, rp, cp, V)
+    assert rr.block_wiedemann_rank(a, b, P, row_precond=rp, col_precond=cp, v=V, ctx=ctx) == r_orc == dense
