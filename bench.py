@@ -1,0 +1,363 @@
+#!/usr/bin/env python
+"""Benchmark of the block-Wiedemann Krylov step on B200.
+
+Workload (the large single-matrix configuration): a 2,000,000 x 1,500,000 CSR
+matrix over p = 2013265921 with 12 distinct Zipf(1.1) columns per row, values
+uniform in [1, p-1] and 10,000 duplicated rows, seeded synthetic data; block
+width b = 16.  One step = one application of B = D_c A^T D_r A D_c (two SpMMs)
+together with the two fused sequence terms S_{2k+1}, S_{2k+2}.
+
+Metric: Krylov SpMM HBM GB/s on the algorithmic byte count per application
+    sum over {A, A^T} of (8 nnz + 4 (rows + 1)) + 4 b 2 (m + n)
+(CSR read once, dense blocks read and written once).  The working set
+(~0.7 GB) is far larger than the 126 MB L2, so no explicit flush is needed.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+N > 1 runs independent replicas (one matrix per GPU, no collective on the
+data path); value is the total over all ranks, time the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+P = 2013265921
+METRIC = "Krylov SpMM HBM GB/s"
+WORKLOAD = "zipf_2000000x1500000_nnz12_b16"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--b", type=int, default=16)
+    ap.add_argument("--small", action="store_true", help="scaled-down workload for quick checks")
+    ap.add_argument("--scale", type=float, default=1.0, help="fraction of the full matrix size (profiling runs)")
+    ap.add_argument("--no-rank", action="store_true", help="skip the rank-pipeline measurement")
+    ap.add_argument("--cpu-samples", type=int, default=6)
+    return ap.parse_args()
+
+
+def workload(small: bool, scale: float = 1.0):
+    from rust_rank_b200 import synth
+
+    if small:
+        scale = 0.1
+    if scale != 1.0:
+        return synth.zipf_large(m=int(2_000_000 * scale), n=int(1_500_000 * scale), k=12,
+                                dup_rows=int(10_000 * scale), p=P, seed=44)
+    return synth.zipf_large(p=P, seed=44)
+
+
+def dist_init(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        self.file.flush()
+        rows = []
+        with open(self.file.name) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for nm, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def cpu_baseline(rowptr, col, val, m, n, b, samples):
+    """The oracle (CPU restatement of the reference's Krylov worker + consumer) on the same matrix."""
+    import oracle
+    from rust_rank_b200 import synth
+
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    dr, dc = synth.preconditioners(m, n, P, 1)
+    V = synth.random_vectors(b, n, P, 2)
+    op = oracle.KrylovOp(rowptr, col, val, m, n, P, dr, dc, V)
+    op.step()  # warm-up
+    t0 = time.perf_counter()
+    for _ in range(samples):
+        op.step()
+    dt = (time.perf_counter() - t0) / samples
+    op.close()
+    bytes_app = 2 * (8.0 * rowptr[-1]) + 4.0 * (m + 1) + 4.0 * (n + 1) + 4.0 * b * 2 * (m + n)
+    return bytes_app / dt / 1e9, dt, threads
+
+
+def run_reference(args):
+    world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return
+    rowptr, col, val, m, n = workload(args.small, args.scale)
+    import oracle
+    from rust_rank_b200 import synth
+
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    dr, dc = synth.preconditioners(m, n, P, 1)
+    V = synth.random_vectors(args.b, n, P, 2)
+    op = oracle.KrylovOp(rowptr, col, val, m, n, P, dr, dc, V)
+    for _ in range(args.warmup):
+        op.step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        op.step()
+    dt = time.perf_counter() - t0
+    bytes_app = 2 * (8.0 * rowptr[-1]) + 4.0 * (m + 1) + 4.0 * (n + 1) + 4.0 * args.b * 2 * (m + n)
+    v = bytes_app * args.steps / dt / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "GB/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32 mod p (u64/u128 accum)",
+        "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD if not args.small else WORKLOAD + "_small", "b": args.b, "p": P,
+                   "l2_policy": "inputs larger than L2"},
+        "cpu_baseline": {"value": v, "unit": "GB/s", "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} applications of B on the full matrix"},
+        "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "CPU restatement of the reference Rust path (the reference cannot be built here: no Rust toolchain)",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def rank_pipeline(ctx, reps=3):
+    """Whole rank computation (Krylov + PM-basis + readout) on the plain single-matrix config."""
+    import rust_rank_b200 as rr
+    from rust_rank_b200 import synth
+
+    rowptr, col, val, m, n = synth.plain_single(n=20000, k=6, dep_rows=500, p=P, seed=43)
+    a = rr.CsrMatrix.from_arrays(rowptr, col, val, m, n)
+    dm = a.to_device(P, ctx)
+    b = 8
+    rp, cp = synth.preconditioners(m, n, P, 5)
+    V = synth.random_vectors(b, n, P, 6)
+    rank = rr.block_wiedemann_rank(dm, b, P, row_precond=rp, col_precond=cp, v=V, ctx=ctx)  # warm-up
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        r = rr.block_wiedemann_rank(dm, b, P, row_precond=rp, col_precond=cp, v=V, ctx=ctx)
+        times.append(time.perf_counter() - t0)
+        assert r == rank
+    med = statistics.median(times)
+    return {"workload": "plain_20000x20000_nnz6_b8 (500 dependent rows)", "rank": rank,
+            "upper_bound_by_construction": m - 500, "ms_per_rank": 1e3 * med, "ranks_per_sec": 1.0 / med,
+            "timing": "wall clock of rr_rank on a resident matrix, median of %d" % reps}
+
+
+def run_engine(args):
+    import torch
+
+    import rust_rank_b200 as rr
+    from rust_rank_b200 import synth
+
+    world, rank, local = dist_init(args.gpus)
+    ctx = rr.Context(local)
+    rowptr, col, val, m, n = workload(args.small, args.scale)
+    b = args.b
+    dr, dc = synth.preconditioners(m, n, P, 1)
+    V = synth.random_vectors(b, n, P, 2)
+    t0 = time.perf_counter()
+    dm = rr.CsrMatrix.from_arrays(rowptr, col, val, m, n).to_device(P, ctx)
+    setup_s = time.perf_counter() - t0
+    ks = rr.KrylovStream(dm, V, dr, dc, 0)
+    bytes_app = ks.bytes_per_application()
+    ks.step_device(args.warmup)
+    ctx.synchronize()
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    launches0 = ks.launch_count()
+    with ClockSampler(local) as clk:
+        barrier(world)
+        ctx.synchronize()
+        e0.record(stream)
+        ks.step_device(args.steps)
+        e1.record(stream)
+        ctx.synchronize()
+        barrier(world)
+    launches = ks.launch_count() - launches0
+    ms = e0.elapsed_time(e1)
+    ms_max = max_over_ranks(ms, world)
+    clocks = clk.summary()
+    value = world * bytes_app * args.steps / (ms_max / 1e3) / 1e9
+
+    # per-phase device times (CUDA events on the context stream, inside the library)
+    ph = ks.profile(max(4, min(args.steps, 10)))
+    pb = ks.phase_bytes()
+    traffic = ncu_traffic()
+    peak, peak_kind = measured_peak()
+    # dominant kernel: the pass over A^T when chunked rows exist is two launches; report each phase
+    phases = {
+        "pass_A": {"ms": ph[0], "alg_bytes": pb[0], "gbs": pb[0] / (ph[0] / 1e3) / 1e9},
+        "pass_At_chunks+rows": {"ms": ph[1] + ph[2], "alg_bytes": pb[1], "gbs": pb[1] / ((ph[1] + ph[2]) / 1e3) / 1e9,
+                                "chunk_ms": ph[1], "rows_ms": ph[2]},
+    }
+    dom = max(phases, key=lambda k: phases[k]["ms"])
+    ach = phases[dom]["gbs"]
+    roof = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+            "peak_kind": peak_kind, "traffic": traffic.get(dom), "phases": phases}
+
+    # e2e: the public API with host buffers (pinned V / preconditioners in, terms + final block out)
+    def pinned(a):
+        return torch.from_numpy(a.view(np.int32)).pin_memory().numpy().view(np.uint32)
+
+    Vp, drp, dcp = pinned(V), pinned(dr), pinned(dc)
+    np_ = b * (b + 1) // 2
+    seq = torch.zeros((np_, 2 * args.steps + 2), dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+    curv_out = torch.zeros((b, n), dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+    barrier(world)
+    t0 = time.perf_counter()
+    ks2 = rr.KrylovStream(dm, Vp, drp, dcp, 0)
+    L = ks2.advance(2 * args.steps, seq)
+    curv_out[:] = ks2.get_curv()
+    e2e_s = time.perf_counter() - t0
+    e2e_s = max_over_ranks(e2e_s, world)
+    assert L == 2 * args.steps + 1
+    ks2.close()
+    e2e = {"value": world * bytes_app * args.steps / e2e_s / 1e9, "unit": "GB/s",
+           "h2d_bytes_per_step": (V.nbytes + dr.nbytes + dc.nbytes) / args.steps,
+           "d2h_bytes_per_step": (4.0 * np_ * L + curv_out.nbytes) / args.steps,
+           "timing": "wall clock over rr_krylov_create + rr_krylov_advance + rr_krylov_get_curv on a resident matrix"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32 mod p (u64 lazy accum)", "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD if (args.scale == 1.0 and not args.small) else f"{WORKLOAD}_scaled", "m": m, "n": n,
+                   "nnz": int(rowptr[-1]), "b": b, "p": P, "parallelism": f"replicas x{world}",
+                   "l2_policy": "inputs larger than L2 (working set ~0.7 GB)"},
+        "roofline": roof, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
+        "matrix_setup_s": setup_s,
+    }
+    if rank == 0 and world == 1 and args.cpu_samples > 0:
+        v, dt, threads = cpu_baseline(rowptr, col, val, m, n, b, args.cpu_samples)
+        line["cpu_baseline"] = {"value": v, "unit": "GB/s", "cores": threads, "kind": "port",
+                                "sample": f"{args.cpu_samples} applications of B (with both sequence terms) on the "
+                                          "full matrix, oracle restatement of the reference CPU path"}
+    if rank == 0 and world == 1 and not args.no_rank:
+        line["rank_pipeline"] = rank_pipeline(ctx)
+    ks.close()
+    dm.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_engine(args)
+
+
+if __name__ == "__main__":
+    main()

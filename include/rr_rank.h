@@ -106,6 +106,16 @@ int rr_krylov_get_curv(rr_krylov* kr, uint32_t* curv);
 /* Algorithmic bytes of one application of B (both SpMMs: CSR read once,
  * dense blocks read and written once), for bandwidth reporting. */
 int rr_krylov_bytes_per_application(const rr_krylov* kr, double* bytes);
+/* The same split by pass: [0] rows of A (8 nnz + 4 (m+1) + 4 b (n + m)),
+ * [1] rows of A^T (8 nnz + 4 (n+1) + 4 b (m + n)). */
+int rr_krylov_phase_bytes(const rr_krylov* kr, double* bytes2);
+/* Like rr_krylov_step_device, but records CUDA events on the context stream
+ * around each phase and returns the mean device time per application in ms:
+ * ms3[0] pass over A (with its chunks), ms3[1] chunks of A^T, ms3[2] pass
+ * over A^T (synchronises). */
+int rr_krylov_profile(rr_krylov* kr, int64_t n_apps, double* ms3);
+/* Number of kernels this handle has launched so far. */
+int rr_krylov_launch_count(const rr_krylov* kr, int64_t* count);
 
 /* ---------------------------------------------------------------- generator */
 /* PM_Basis (src/sigma_basis.rs:9-54): minimal matrix generator of the

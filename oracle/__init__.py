@@ -41,9 +41,12 @@ def lib():
         L.orc_krylov.restype = _i64
         L.orc_krylov.argtypes = [_i64, _i64, _i64p, _i32p, _u32p, C.c_uint32, C.c_int, _u32p, _u32p, _u32p,
                                  _i64, _i64, _u32p, _i64]
-        L.orc_apply_b.restype = C.c_int
-        L.orc_apply_b.argtypes = [_i64, _i64, _i64p, _i32p, _u32p, _i64p, _i32p, _u32p, C.c_uint32, C.c_int,
-                                  _u32p, _u32p, _u32p, _u32p]
+        L.orc_op_create.restype = C.c_void_p
+        L.orc_op_create.argtypes = [_i64, _i64, _i64p, _i32p, _u32p, C.c_uint32, C.c_int, _u32p, _u32p, _u32p]
+        L.orc_op_step.restype = C.c_int
+        L.orc_op_step.argtypes = [C.c_void_p, _u32p, _u32p]
+        L.orc_op_destroy.restype = None
+        L.orc_op_destroy.argtypes = [C.c_void_p]
         L.orc_lsp.argtypes = [C.c_int, _u64p, C.c_uint64, _u64p, _u64p, _i32p]
         L.orc_matrix_inverse.argtypes = [C.c_int, _u64p, C.c_uint64, _u64p]
         L.orc_modular_rank.restype = _i64
@@ -106,6 +109,33 @@ def krylov(rowptr, col, val, m, n, p, row_precond, col_precond, curv, seq_len, m
     if new_len < 0:
         raise ValueError("oracle krylov: bad arguments")
     return out[:, :new_len], new_len, cv
+
+
+class KrylovOp:
+    """One application of B at a time (for timing the CPU baseline)."""
+
+    def __init__(self, rowptr, col, val, m, n, p, row_precond, col_precond, curv):
+        self.b = curv.shape[0]
+        self.np = self.b * (self.b + 1) // 2
+        self.h = lib().orc_op_create(m, n, np.ascontiguousarray(rowptr, np.int64), np.ascontiguousarray(col, np.int32),
+                                     np.ascontiguousarray(val, np.uint32), p, self.b,
+                                     np.ascontiguousarray(row_precond, np.uint32),
+                                     np.ascontiguousarray(col_precond, np.uint32),
+                                     np.ascontiguousarray(curv, np.uint32))
+
+    def step(self):
+        g1 = np.zeros(self.np, np.uint32)
+        g2 = np.zeros(self.np, np.uint32)
+        lib().orc_op_step(self.h, g1, g2)
+        return g1, g2
+
+    def close(self):
+        if self.h:
+            lib().orc_op_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
 
 
 # ---------------------------------------------------------------- generator

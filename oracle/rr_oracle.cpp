@@ -493,29 +493,54 @@ i64 orc_krylov(i64 m, i64 n, const i64* rowptr, const int32_t* col, const uint32
   return len;
 }
 
-// One B application on an interleaved block, without the Gram terms: used by
-// the CPU baseline timing.  x_in / x_out are n x b interleaved.
-int orc_apply_b(i64 m, i64 n, const i64* rowptr, const int32_t* col, const uint32_t* scaled_val,
-                const i64* trowptr, const int32_t* tcol, const uint32_t* tscaled_val, uint32_t p, int b,
-                const uint32_t* x_in, uint32_t* x_out, uint32_t* gram_odd, uint32_t* gram_even) {
+// The same Krylov step as orc_krylov, split so the CPU baseline can time
+// individual applications of B: orc_op_create prepares a = D_r A D_c and
+// at = D_c A^T once (src/main.rs:522-526); orc_op_step runs one worker
+// iteration plus the consumer's two dot-product terms (src/vectorstream.rs:63-64,
+// src/main.rs:138-156) on an interleaved block x (n x b), in place.
+struct OrcOp {
   Csr a, at;
-  a.rows = m; a.cols = n;
-  a.ptr.assign(rowptr, rowptr + m + 1);
-  a.idx.assign(col, col + rowptr[m]);
-  a.val.assign(scaled_val, scaled_val + rowptr[m]);
-  at.rows = n; at.cols = m;
-  at.ptr.assign(trowptr, trowptr + n + 1);
-  at.idx.assign(tcol, tcol + trowptr[n]);
-  at.val.assign(tscaled_val, tscaled_val + trowptr[n]);
-  std::vector<u64> x(x_in, x_in + (size_t)n * b), y, w, g;
-  spmm(a, x, y, b, p);
-  spmm(at, y, w, b, p);
-  const int np = b * (b + 1) / 2;
-  if (gram_odd) { gram_pairs(x, w, n, b, p, g); for (int q = 0; q < np; ++q) gram_odd[q] = (uint32_t)g[q]; }
-  if (gram_even) { gram_pairs(w, w, n, b, p, g); for (int q = 0; q < np; ++q) gram_even[q] = (uint32_t)g[q]; }
-  for (size_t i = 0; i < w.size(); ++i) x_out[i] = (uint32_t)w[i];
+  u64 p;
+  int b;
+  std::vector<u64> x, y, w, g;
+};
+
+void* orc_op_create(i64 m, i64 n, const i64* rowptr, const int32_t* col, const uint32_t* val, uint32_t p, int b,
+                    const uint32_t* row_precond, const uint32_t* col_precond, const uint32_t* curv) {
+  OrcOp* op = new OrcOp;
+  op->p = p;
+  op->b = b;
+  op->a.rows = m;
+  op->a.cols = n;
+  op->a.ptr.assign(rowptr, rowptr + m + 1);
+  op->a.idx.assign(col, col + rowptr[m]);
+  op->a.val.assign(val, val + rowptr[m]);
+  op->at = transpose(op->a);
+  for (i64 r = 0; r < m; ++r)
+    for (i64 k = op->a.ptr[r]; k < op->a.ptr[r + 1]; ++k)
+      op->a.val[k] = mulmod(mulmod(op->a.val[k], row_precond[r], p), col_precond[op->a.idx[k]], p);
+  for (i64 c = 0; c < n; ++c)
+    for (i64 k = op->at.ptr[c]; k < op->at.ptr[c + 1]; ++k) op->at.val[k] = mulmod(op->at.val[k], col_precond[c], p);
+  op->x.resize((size_t)n * b);
+  for (int l = 0; l < b; ++l)
+    for (i64 c = 0; c < n; ++c) op->x[(size_t)c * b + l] = curv[(size_t)l * n + c] % p;
+  return op;
+}
+
+int orc_op_step(void* h, uint32_t* gram_odd, uint32_t* gram_even) {
+  OrcOp* op = static_cast<OrcOp*>(h);
+  const int b = op->b, np = b * (b + 1) / 2;
+  spmm(op->a, op->x, op->y, b, op->p);
+  spmm(op->at, op->y, op->w, b, op->p);
+  gram_pairs(op->x, op->w, op->a.cols, b, op->p, op->g);
+  for (int q = 0; q < np; ++q) gram_odd[q] = (uint32_t)op->g[q];
+  gram_pairs(op->w, op->w, op->a.cols, b, op->p, op->g);
+  for (int q = 0; q < np; ++q) gram_even[q] = (uint32_t)op->g[q];
+  op->x.swap(op->w);
   return 0;
 }
+
+void orc_op_destroy(void* h) { delete static_cast<OrcOp*>(h); }
 
 // src/modular_linalg.rs:188-239.  a, L, S are m x m row-major; perm gets the
 // column permutation (perm[i] = original column now at position i).

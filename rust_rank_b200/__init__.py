@@ -188,6 +188,22 @@ class KrylovStream:
         check(lib().rr_krylov_bytes_per_application(self.handle, C.byref(v)))
         return v.value
 
+    def phase_bytes(self):
+        v = (C.c_double * 2)()
+        check(lib().rr_krylov_phase_bytes(self.handle, v))
+        return v[0], v[1]
+
+    def profile(self, n_apps: int):
+        """Mean device ms per application: (pass over A, chunks of A^T, pass over A^T)."""
+        v = (C.c_double * 3)()
+        check(lib().rr_krylov_profile(self.handle, int(n_apps), v))
+        return v[0], v[1], v[2]
+
+    def launch_count(self) -> int:
+        v = C.c_int64()
+        check(lib().rr_krylov_launch_count(self.handle, C.byref(v)))
+        return v.value
+
     def close(self):
         if getattr(self, "handle", None):
             lib().rr_krylov_destroy(self.handle)

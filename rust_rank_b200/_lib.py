@@ -42,6 +42,9 @@ SIGNATURES = {
     "rr_krylov_length": (C.c_int, [_vp, _pi64]),
     "rr_krylov_get_curv": (C.c_int, [_vp, _vp]),
     "rr_krylov_bytes_per_application": (C.c_int, [_vp, C.POINTER(C.c_double)]),
+    "rr_krylov_phase_bytes": (C.c_int, [_vp, C.POINTER(C.c_double)]),
+    "rr_krylov_profile": (C.c_int, [_vp, _i64, C.POINTER(C.c_double)]),
+    "rr_krylov_launch_count": (C.c_int, [_vp, _pi64]),
     "rr_pm_basis": (C.c_int, [_vp, _vp, _i64, _i32, _i64, _i64, _u32, _vp, _vp]),
     "rr_rank_from_basis": (C.c_int, [_vp, _vp, _i32, _i64, _u32, _pi64]),
     "rr_rank": (C.c_int, [_vp, _i32, _vp, _vp, _vp, _i64, _pi64]),

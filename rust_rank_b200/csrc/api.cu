@@ -286,7 +286,7 @@ int rr_krylov_destroy(rr_krylov* kr) {
 static int queue_apps(rr_krylov* kr, int64_t n_apps) {
   if (kr->len == 0) kr->len = 1;  // publish S_0
   RR_TRY(ensure_capacity(kr, kr->len - kr->base + 2 * n_apps + 1));
-  for (int64_t i = 0; i < n_apps; ++i) RR_TRY(krylov_launch_application(kr));
+  for (int64_t i = 0; i < n_apps; ++i) RR_TRY(krylov_launch_application(kr, nullptr));
   return RR_OK;
 }
 
@@ -355,6 +355,47 @@ int rr_krylov_bytes_per_application(const rr_krylov* kr, double* bytes) {
   const rr_matrix* m = kr->mat;
   const double csr = 2.0 * (8.0 * (double)m->nnz) + 4.0 * ((double)m->m + 1) + 4.0 * ((double)m->n + 1);
   *bytes = csr + 4.0 * kr->b * 2.0 * ((double)m->m + (double)m->n);
+  return RR_OK;
+}
+
+int rr_krylov_phase_bytes(const rr_krylov* kr, double* bytes2) {
+  if (!kr || !bytes2) return fail(RR_EINVAL, "NULL argument");
+  const rr_matrix* m = kr->mat;
+  const double dense = 4.0 * kr->b * ((double)m->m + (double)m->n);
+  bytes2[0] = 8.0 * (double)m->nnz + 4.0 * ((double)m->m + 1) + dense;
+  bytes2[1] = 8.0 * (double)m->nnz + 4.0 * ((double)m->n + 1) + dense;
+  return RR_OK;
+}
+
+int rr_krylov_profile(rr_krylov* kr, int64_t n_apps, double* ms3) {
+  if (!kr || !ms3 || n_apps < 1) return fail(RR_EINVAL, "bad argument");
+  RR_CUDA(cudaSetDevice(kr->mat->ctx->device));
+  if (kr->len == 0) kr->len = 1;
+  RR_TRY(ensure_capacity(kr, kr->len - kr->base + 2 * n_apps + 1));
+  std::vector<cudaEvent_t> ev((size_t)4 * n_apps, nullptr);
+  int status = RR_OK;
+  for (auto& e : ev)
+    if (cudaEventCreate(&e) != cudaSuccess) { status = fail(RR_ECUDA, "cudaEventCreate failed"); break; }
+  for (int64_t i = 0; i < n_apps && status == RR_OK; ++i) status = krylov_launch_application(kr, &ev[(size_t)4 * i]);
+  double acc[3] = {0, 0, 0};
+  if (status == RR_OK && cudaStreamSynchronize(kr->mat->ctx->stream) != cudaSuccess)
+    status = fail(RR_ECUDA, "stream synchronize failed: %s", cudaGetErrorString(cudaGetLastError()));
+  for (int64_t i = 0; i < n_apps && status == RR_OK; ++i)
+    for (int k = 0; k < 3; ++k) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, ev[(size_t)4 * i + k], ev[(size_t)4 * i + k + 1]);
+      acc[k] += ms;
+    }
+  for (auto& e : ev)
+    if (e) cudaEventDestroy(e);
+  if (status != RR_OK) return status;
+  for (int k = 0; k < 3; ++k) ms3[k] = acc[k] / (double)n_apps;
+  return RR_OK;
+}
+
+int rr_krylov_launch_count(const rr_krylov* kr, int64_t* count) {
+  if (!kr || !count) return fail(RR_EINVAL, "NULL argument");
+  *count = kr->launches;
   return RR_OK;
 }
 

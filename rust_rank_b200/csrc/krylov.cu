@@ -337,6 +337,7 @@ static int launch_pass_B(rr_krylov* kr, const PassParams& P, int mode) {
 }
 
 static int launch_pass(rr_krylov* kr, const PassParams& P, int mode) {
+  kr->launches += 1;
   switch (kr->B) {
     case 4: return launch_pass_B<4>(kr, P, mode);
     case 8: return launch_pass_B<8>(kr, P, mode);
@@ -357,6 +358,7 @@ static int launch_chunk_B(rr_krylov* kr, const ChunkParams& P) {
 }
 
 static int launch_chunk(rr_krylov* kr, const ChunkParams& P) {
+  kr->launches += 1;
   switch (kr->B) {
     case 4: return launch_chunk_B<4>(kr, P);
     case 8: return launch_chunk_B<8>(kr, P);
@@ -432,11 +434,15 @@ static int run_chunks(rr_krylov* kr, const DevCsr& A, const uint32_t* X) {
   return launch_chunk(kr, C);
 }
 
-int krylov_launch_application(rr_krylov* kr) {
+// ev (optional): four events recorded before pass 1, after pass 1, after the
+// chunks of pass 2 and after pass 2.
+int krylov_launch_application(rr_krylov* kr, cudaEvent_t* ev) {
   const int np = kr->b * (kr->b + 1) / 2;
   rr_matrix* mat = kr->mat;
+  cudaStream_t s = mat->ctx->stream;
   uint32_t* x = kr->X[kr->cur].ptr;
   uint32_t* xn = kr->X[kr->cur ^ 1].ptr;
+  if (ev) RR_CUDA(cudaEventRecord(ev[0], s));
   // pass 1: rows of A
   RR_TRY(run_chunks(kr, mat->A, x));
   PassParams P = base_params(kr);
@@ -450,8 +456,10 @@ int krylov_launch_application(rr_krylov* kr) {
   P.scale = kr->dr.ptr;
   P.S_out = kr->S.ptr + (size_t)(kr->len - kr->base) * np;
   RR_TRY(launch_pass(kr, P, kModeOdd));
+  if (ev) RR_CUDA(cudaEventRecord(ev[1], s));
   // pass 2: rows of A^T
   RR_TRY(run_chunks(kr, mat->At, kr->U.ptr));
+  if (ev) RR_CUDA(cudaEventRecord(ev[2], s));
   P.rowptr = mat->At.rowptr.ptr;
   P.col = mat->At.col.ptr;
   P.val = mat->At.val.ptr;
@@ -462,6 +470,7 @@ int krylov_launch_application(rr_krylov* kr) {
   P.scale = kr->dc.ptr;
   P.S_out = kr->S.ptr + (size_t)(kr->len + 1 - kr->base) * np;
   RR_TRY(launch_pass(kr, P, kModeEven));
+  if (ev) RR_CUDA(cudaEventRecord(ev[3], s));
   kr->len += 2;
   kr->cur ^= 1;
   return RR_OK;

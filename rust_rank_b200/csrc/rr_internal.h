@@ -121,11 +121,12 @@ struct rr_krylov_s {
   int64_t len = 0;  // terms queued so far
   int cur = 0;      // index of the current X
   int grid_pass = 0, grid_chunk = 0;
+  int64_t launches = 0;  // kernels launched by this handle
 };
 
 namespace rr {
 int krylov_launch_init(rr_krylov* kr, const uint32_t* d_w, bool emit_s0);
-int krylov_launch_application(rr_krylov* kr);
+int krylov_launch_application(rr_krylov* kr, cudaEvent_t* ev);
 int krylov_launch_get_curv(rr_krylov* kr, uint32_t* d_out);
 int krylov_occupancy(rr_krylov* kr);
 int matrix_build(rr_ctx* ctx, int64_t m, int64_t n, const int64_t* rowptr, const int32_t* col,
