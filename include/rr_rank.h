@@ -126,6 +126,24 @@ int rr_krylov_launch_count(const rr_krylov* kr, int64_t* count);
  * p = 2013265921 = 15*2^27+1 up to d = 2^26). */
 int rr_pm_basis(rr_ctx* ctx, const uint32_t* seq, int64_t seq_stride, int32_t b, int64_t nlen, int64_t d,
                 uint32_t p, uint32_t* M, int64_t* delta);
+/* No counterpart in the reference.  PM-basis of a short sequence for callers
+ * that cannot allocate device memory: code running while a CUDA stream is
+ * being captured into a graph, runtimes that hand all device memory to their
+ * own pool allocator, or latency-critical loops where cudaMalloc's implicit
+ * synchronisation is not acceptable.  Same result as rr_pm_basis, but every
+ * pointer is DEVICE memory owned by the caller: d_seq[b(b+1)/2][seq_stride]
+ * (nlen valid terms), d_M[2b][2b][d'+1] and d_delta[2b] (d' = d rounded up to a
+ * power of two).  Limits: 1 <= b <= 16 and d' <= 32 (RR_EINVAL beyond them).
+ * The work is queued on `stream` (a cudaStream_t; NULL = legacy default) and
+ * the call returns without waiting; outputs are ready when the stream gets
+ * there.  Scratch is one fixed 338,176-byte __device__ array inside the
+ * library, present on every GPU that loads it until the process exits; the
+ * first call on a device looks up its address (make that first call before
+ * any stream capture).  All calls share that array: calls whose work can
+ * overlap on the GPU (different streams, different host threads) race and
+ * must be serialised by the caller. */
+int rr_pm_basis_short_noalloc(const uint32_t* d_seq, int64_t seq_stride, int32_t b, int64_t nlen, int64_t d,
+                              uint32_t p, uint32_t* d_M, int64_t* d_delta, void* stream);
 /* analyze_pm_basis + analyze_min_generators (src/sigma_basis.rs:71-152,
  * src/blockbmtest.rs:574-599): rank = b*(k-3) + rank(P[k-1]) + rank(P[0]).
  * M[2b][2b][len].  RR_ESTATE when k < 3 (no estimate). */

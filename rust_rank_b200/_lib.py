@@ -46,6 +46,7 @@ SIGNATURES = {
     "rr_krylov_profile": (C.c_int, [_vp, _i64, C.POINTER(C.c_double)]),
     "rr_krylov_launch_count": (C.c_int, [_vp, _pi64]),
     "rr_pm_basis": (C.c_int, [_vp, _vp, _i64, _i32, _i64, _i64, _u32, _vp, _vp]),
+    "rr_pm_basis_short_noalloc": (C.c_int, [_vp, _i64, _i32, _i64, _i64, _u32, _vp, _vp, _vp]),
     "rr_rank_from_basis": (C.c_int, [_vp, _vp, _i32, _i64, _u32, _pi64]),
     "rr_rank": (C.c_int, [_vp, _i32, _vp, _vp, _vp, _i64, _pi64]),
     "rr_wdm_save": (C.c_int, [C.c_char_p, _i64, _i64, _u32, _i32, _vp, _vp, _vp, _vp, _vp, _i64, _i64]),

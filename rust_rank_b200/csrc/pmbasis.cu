@@ -34,6 +34,7 @@
 #include <algorithm>
 #include <cstring>
 #include <memory>
+#include <mutex>
 
 #include "rr_internal.h"
 
@@ -686,4 +687,98 @@ int pm_basis_device(rr_ctx* ctx, const uint32_t* seq, int64_t seq_stride, int b,
   return RR_OK;
 }
 
+// ---------------------------------------------------------------- no-allocation variant
+// rr_pm_basis_short_noalloc runs the same two kernels as rr_pm_basis does for a
+// short sequence (build_G_kernel, then one pm_base_kernel block), but takes its
+// scratch -- the matrix G, the base kernel's double-buffered basis and the
+// status word -- from the file-scope array below instead of allocating it.
+// Limits: b <= 16 and d (rounded up to a power of two) <= 32.
+namespace {
+constexpr int kNoallocMaxB = 16;
+constexpr int kNoallocMaxD = 32;
+constexpr size_t round256(size_t x) { return (x + 255) & ~(size_t)255; }
+constexpr size_t kNaGOff = 0;
+constexpr size_t kNaGBytes = round256((size_t)2 * kNoallocMaxB * kNoallocMaxB * (kNoallocMaxD + 1) * 4);
+constexpr size_t kNaMbufOff = kNaGOff + kNaGBytes;
+constexpr size_t kNaMbufBytes =
+    round256((size_t)2 * (kNoallocMaxD + 1) * (2 * kNoallocMaxB) * (2 * kNoallocMaxB) * 4);
+constexpr size_t kNaStatusOff = kNaMbufOff + kNaMbufBytes;
+constexpr size_t kNoallocScratchBytes = kNaStatusOff + 256;  // 338,176 bytes
+constexpr int kNoallocMaxDevices = 64;
+
+std::mutex g_noalloc_mutex;
+unsigned char* g_noalloc_addr[kNoallocMaxDevices] = {};
+}  // namespace
+
+// Held by every GPU that loads this library, until the process exits.
+static __device__ __align__(256) unsigned char g_pm_noalloc_scratch[kNoallocScratchBytes];
+
+// Device address of the scratch array on the current device, looked up once
+// per device (host code must not use the symbol itself as an address).
+static int noalloc_scratch(unsigned char** out) {
+  int dev = 0;
+  RR_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoallocMaxDevices) return fail(RR_EUNSUPPORTED, "device %d beyond %d", dev, kNoallocMaxDevices);
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    RR_CUDA(cudaGetSymbolAddress(&p, g_pm_noalloc_scratch));
+    g_noalloc_addr[dev] = static_cast<unsigned char*>(p);
+  }
+  *out = g_noalloc_addr[dev];
+  return RR_OK;
+}
+
 }  // namespace rr
+
+extern "C" int rr_pm_basis_short_noalloc(const uint32_t* d_seq, int64_t seq_stride, int32_t b, int64_t nlen, int64_t d,
+                                         uint32_t p, uint32_t* d_M, int64_t* d_delta, void* stream) {
+  using namespace rr;
+  if (!d_seq || !d_M || !d_delta) return fail(RR_EINVAL, "NULL argument");
+  RR_TRY(rr_prime_check(p));
+  if (b < 1 || b > kNoallocMaxB)
+    return fail(RR_EINVAL, "b = %d outside the no-allocation limit 1 <= b <= %d", b, kNoallocMaxB);
+  if (d < 1) return fail(RR_EINVAL, "d = %lld must be >= 1", (long long)d);
+  int64_t dd = 1;
+  while (dd < d) dd *= 2;
+  if (dd > kNoallocMaxD)
+    return fail(RR_EINVAL, "d = %lld (rounded to %lld) exceeds the no-allocation limit d <= %d; use rr_pm_basis",
+                (long long)d, (long long)dd, kNoallocMaxD);
+  if (dd >= nlen) return fail(RR_EINVAL, "sequence too short: d = %lld, nlen = %lld", (long long)dd, (long long)nlen);
+  if (seq_stride < nlen) return fail(RR_EINVAL, "seq_stride < nlen");
+  unsigned char* base = nullptr;
+  RR_TRY(noalloc_scratch(&base));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int m = 2 * b, n = b;
+  const int64_t glen = dd + 1;
+  uint32_t* G = reinterpret_cast<uint32_t*>(base + kNaGOff);
+  uint32_t* Mbuf = reinterpret_cast<uint32_t*>(base + kNaMbufOff);
+  int* status = reinterpret_cast<int*>(base + kNaStatusOff);
+  // delta starts at zero (src/sigma_basis.rs:48); the status word is cleared per call
+  RR_CUDA(cudaMemsetAsync(d_delta, 0, (size_t)m * sizeof(int64_t), s));
+  RR_CUDA(cudaMemsetAsync(status, 0, sizeof(int), s));
+  build_G_kernel<<<grid_for((int64_t)m * n * glen), 256, 0, s>>>(d_seq, seq_stride, b, glen, G, p);
+  RR_CUDA(cudaGetLastError());
+  BaseParams B;
+  B.G = G;
+  B.g_rs = (int64_t)n * glen;
+  B.g_cs = glen;
+  B.m = m;
+  B.n = n;
+  B.nleaves = (int)dd;
+  B.delta = d_delta;
+  B.Mout = d_M;
+  B.out_rs = (int64_t)m * glen;
+  B.out_cs = glen;
+  B.Mbuf = Mbuf;
+  B.M = make_modp(p);
+  B.status = status;
+  const int K = (int)dd;
+  size_t words = (size_t)2 * K * m * n + (size_t)m * (n + m) + (size_t)m * m + 3 * (size_t)m + 1;
+  size_t bytes = (words * 4 + 7) & ~(size_t)7;
+  bytes += 2 * (size_t)m * 8 + 3 * (size_t)m * 4 + 64;
+  RR_CUDA(cudaFuncSetAttribute(pm_base_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  pm_base_kernel<<<1, kBaseThreads, bytes, s>>>(B);
+  RR_CUDA(cudaGetLastError());
+  return RR_OK;
+}
