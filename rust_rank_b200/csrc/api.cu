@@ -56,6 +56,10 @@ ModP make_modp(uint32_t p) {
   M.p = p;
   M.c32 = (uint32_t)((((uint64_t)1) << 32) % p);
   M.mu = (uint64_t)(~0ull) / p;  // floor((2^64 - 1) / p) == floor(2^64 / p) for odd p
+  uint32_t inv = p;              // Newton iteration for p^{-1} mod 2^32 (p odd)
+  for (int i = 0; i < 5; ++i) inv *= 2u - p * inv;
+  M.pinv = (uint32_t)(0u - inv);
+  M.r1 = M.c32;
   return M;
 }
 
@@ -239,12 +243,24 @@ int rr_krylov_create(rr_matrix* mat, int32_t b, const uint32_t* row_precond, con
       inv = inv * dc[i] % p;
     }
   }
-  RR_TRY(kr->dr.alloc(m));
-  RR_TRY(kr->dc.alloc(n));
-  RR_TRY(kr->dcinv.alloc(n));
-  RR_CUDA(cudaMemcpyAsync(kr->dr.ptr, dr.data(), m * 4, cudaMemcpyHostToDevice, s));
-  RR_CUDA(cudaMemcpyAsync(kr->dc.ptr, dc.data(), n * 4, cudaMemcpyHostToDevice, s));
-  RR_CUDA(cudaMemcpyAsync(kr->dcinv.ptr, dci.data(), n * 4, cudaMemcpyHostToDevice, s));
+  {
+    const uint64_t R1 = kr->M.r1, R2 = R1 * R1 % p;
+    std::vector<uint32_t> dcr(n);
+    for (int64_t i = 0; i < m; ++i) dr[i] = (uint32_t)(dr[i] * R2 % p);
+    for (int64_t i = 0; i < n; ++i) {
+      dcr[i] = (uint32_t)(dc[i] * R1 % p);
+      dc[i] = (uint32_t)(dc[i] * R2 % p);
+    }
+    RR_TRY(kr->dr_m.alloc(m));
+    RR_TRY(kr->dc_m.alloc(n));
+    RR_TRY(kr->dc_r.alloc(n));
+    RR_TRY(kr->dcinv.alloc(n));
+    RR_CUDA(cudaMemcpyAsync(kr->dr_m.ptr, dr.data(), m * 4, cudaMemcpyHostToDevice, s));
+    RR_CUDA(cudaMemcpyAsync(kr->dc_m.ptr, dc.data(), n * 4, cudaMemcpyHostToDevice, s));
+    RR_CUDA(cudaMemcpyAsync(kr->dc_r.ptr, dcr.data(), n * 4, cudaMemcpyHostToDevice, s));
+    RR_CUDA(cudaMemcpyAsync(kr->dcinv.ptr, dci.data(), n * 4, cudaMemcpyHostToDevice, s));
+    RR_CUDA(cudaStreamSynchronize(s));  // host vectors die at scope end
+  }
   const int B = kr->B;
   RR_TRY(kr->X[0].alloc((size_t)n * B));
   RR_TRY(kr->X[1].alloc((size_t)n * B));

@@ -13,21 +13,29 @@
 //   pass 1 (rows of A):   z = A x;  U = D_r z;  Gram_odd  += z (x) U
 //   pass 2 (rows of A^T): t = A^T U; w' = D_c t; x' = D_c w';  Gram_even += w' (x) w'
 //
-// The block is stored interleaved, X[row][B] uint32 (B = 4..32 lanes), so a
-// gathered row is one 16..128-byte segment read by B/4 threads with 128-bit
-// loads.  Sums are accumulated lazily in 64 bits with a fold every 2 or 4
-// products (rr_modp.cuh).  The Gram terms are reduced per CTA in shared
-// memory, then across CTAs with 64-bit atomics; the last CTA to finish writes
-// the finished term and resets the accumulators, so no separate reduction
-// kernel and no host round trip is needed.
+// The block is stored interleaved, X[row][B] uint32 (B = 4..32 lanes); a
+// thread owns 8 lanes (4 when B = 4) and gathers them with 128-bit loads, so a
+// row of the block is one 16..128-byte segment.  CSR entries are packed
+// (column, value) pairs read with one 64-bit load.  Each thread issues the
+// loads of four entries before it multiplies, so eight (or four) gathers are in
+// flight per thread.  Sums are accumulated lazily in 64 bits with a fold every
+// 2 or 4 products and finished with a Montgomery reduction; the factor R^{-1}
+// it leaves is absorbed into the preconditioner scales (d R^2 mod p, d R mod p)
+// and, for the odd term, into one final multiplication by R.
 //
-// Rows are renumbered by decreasing degree.  Rows longer than kHeavyDegree
-// (Zipf-heavy columns of A^T) are cut into chunks of kChunkNnz entries that
-// are processed warp-per-chunk and merged with 64-bit atomics; the pass
-// kernel then applies the epilogue to them like to any other row.
+// The Gram terms are reduced per CTA in shared memory, then across CTAs with
+// 64-bit atomics; the last CTA to finish writes the finished term and resets
+// the accumulators, so no separate reduction kernel and no host round trip is
+// needed.
+//
+// Rows are renumbered by decreasing degree.  Rows longer than kHeavyDegree are
+// cut into chunks of at most kChunkNnz entries that are processed
+// warp-per-chunk and merged with 64-bit atomics; the pass kernel then applies
+// the epilogue to them like to any other row.
 #include <algorithm>
 #include <cstring>
 #include <numeric>
+#include <type_traits>
 
 #include "rr_internal.h"
 
@@ -37,24 +45,25 @@ enum PassMode { kModeInit = 0, kModeOdd = 1, kModeEven = 2 };
 
 struct PassParams {
   const uint32_t* rowptr;
-  const int32_t* col;
-  const uint32_t* val;
+  const uint2* cv;          // packed (column, value)
   int64_t rows;
   int64_t heavy_rows;
   const uint4* X;           // gathered block [cols][B/4]   (kModeInit: w [rows][B/4])
   uint4* Y;                 // output block   [rows][B/4]
-  const uint32_t* scale;    // per-row diagonal: d_r (odd), d_c (even, init)
+  const uint32_t* scale;    // odd: d_r R^2; even: d_c R^2; init: d_c R   (all mod p)
+  const uint32_t* scale2;   // even: d_c R
   unsigned long long* heavy_acc;  // [heavy_rows][B]
   unsigned long long* gram_acc;   // [B(B+1)/2]
   unsigned int* counter;
   uint32_t* S_out;          // finished term, real pairs; nullptr = do not emit
+  uint32_t gram_mul;        // factor applied to the finished term
+  uint32_t w4, w5, w6;      // 2^32, 2^40, 2^48 mod p (limb weights of the tensor-core Gram)
   int b_real;
   ModP M;
 };
 
 struct ChunkParams {
-  const int32_t* col;
-  const uint32_t* val;
+  const uint2* cv;
   const uint32_t* chunk_row;
   const uint32_t* chunk_begin;
   const uint32_t* chunk_end;
@@ -67,6 +76,14 @@ struct ChunkParams {
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 
+template <int B>
+struct Shape {
+  static constexpr int LPT = (B >= 8) ? 8 : 4;  // lanes of the block per thread
+  static constexpr int NV = LPT / 4;             // 128-bit words per thread per row
+  static constexpr int TPR = B / LPT;            // threads per row
+  static constexpr int RPW = 32 / TPR;           // rows per warp batch (slots)
+};
+
 __device__ __forceinline__ void pair_of(int q, int B, int& i, int& j) {
   // q enumerates (i <= j) row-major: offset(i) = i*B - i*(i-1)/2
   i = 0;
@@ -78,15 +95,308 @@ __device__ __forceinline__ void pair_of(int q, int B, int& i, int& j) {
   j = i + (q - off);
 }
 
+// acc[l] += sum over entries k = beg, beg+stride, ... < end of val * X[col][lane l]
+// for this thread's LPT lanes (lane block `sub`).  Four entries per step, all
+// loads issued before the multiplies; acc is folded after every FE products,
+// so it leaves folded (< p * 2^32).
+template <int B, int FE>
+__device__ __forceinline__ void mac_step(const uint2 (&e)[4], const uint4 (&g)[4][Shape<B>::NV], const ModP& M,
+                                         uint64_t (&acc)[Shape<B>::LPT]) {
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const uint32_t val = e[u].y;
+#pragma unroll
+    for (int v = 0; v < Shape<B>::NV; ++v) {
+      acc[4 * v + 0] = mad_wide(val, g[u][v].x, acc[4 * v + 0]);
+      acc[4 * v + 1] = mad_wide(val, g[u][v].y, acc[4 * v + 1]);
+      acc[4 * v + 2] = mad_wide(val, g[u][v].z, acc[4 * v + 2]);
+      acc[4 * v + 3] = mad_wide(val, g[u][v].w, acc[4 * v + 3]);
+    }
+    if ((u % FE) == FE - 1) {
+#pragma unroll
+      for (int l = 0; l < Shape<B>::LPT; ++l) acc[l] = fold(acc[l], M);
+    }
+  }
+}
+
+// Full steps of four entries run without predicates, with the entries of the
+// next step loaded while the current step's gathers are in flight; the last,
+// partial step clamps its index into the row and multiplies by zero instead
+// of branching (the clamped gather re-reads a row already in cache).
+template <int B, int FE>
+__device__ __forceinline__ void gather_sum(const uint2* __restrict__ cv, uint32_t beg, uint32_t end, uint32_t stride,
+                                           const uint4* __restrict__ X, int sub, const ModP& M,
+                                           uint64_t (&acc)[Shape<B>::LPT]) {
+  constexpr int NV = Shape<B>::NV;
+  constexpr int RW = B / 4;  // 128-bit words per block row
+  const uint4* Xs = X + sub * NV;
+  uint32_t k = beg;
+  const uint32_t step = 4 * stride;
+  if (k + 3 * stride < end) {
+    uint2 e[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) e[u] = __ldg(cv + k + u * stride);
+    for (;;) {
+      uint4 g[4][NV];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < NV; ++v) g[u][v] = __ldg(Xs + (size_t)e[u].x * RW + v);
+      k += step;
+      const bool more = k + 3 * stride < end;
+      uint2 en[4];
+      if (more) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) en[u] = __ldg(cv + k + u * stride);
+      }
+      mac_step<B, FE>(e, g, M, acc);
+      if (!more) break;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) e[u] = en[u];
+    }
+  }
+  if (k < end) {
+    uint2 e[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const uint32_t kk = k + u * stride;
+      e[u] = __ldg(cv + (kk < end ? kk : k));
+      if (kk >= end) e[u].y = 0u;
+    }
+    uint4 g[4][NV];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) g[u][v] = __ldg(Xs + (size_t)e[u].x * RW + v);
+    mac_step<B, FE>(e, g, M, acc);
+  }
+}
+
+__device__ __forceinline__ int pair_index(int i, int j, int B) { return i * B - i * (i - 1) / 2 + (j - i); }
+
+// ---------------------------------------------------------------- Gram terms
+// Both accumulators sum G[i][j] = sum over rows of gz[i] * gu[j] (i <= j) for
+// the rows a warp processes, then add their residues into the CTA's red[].
+
+// CUDA cores (B = 4): the batch is staged in shared memory and every lane
+// accumulates a few (i, j) pairs over the staged rows.
+template <int B, int FE>
+struct GramCore {
+  static constexpr int LPT = Shape<B>::LPT, RPW = Shape<B>::RPW;
+  static constexpr int NP = B * (B + 1) / 2, PPL = (NP + 31) / 32;
+  static constexpr int kWords = 2 * RPW * B;  // shared words per warp
+  uint32_t* zs;  // [RPW][B]
+  uint32_t* us;
+  uint32_t pij[PPL];
+  unsigned long long acc[PPL];
+
+  __device__ __forceinline__ void init(uint32_t* w, int lane) {
+    zs = w;
+    us = w + RPW * B;
+#pragma unroll
+    for (int t = 0; t < PPL; ++t) {
+      const int q = lane + 32 * t;
+      int i = 0, j = 0;
+      if (q < NP) pair_of(q, B, i, j);
+      pij[t] = ((uint32_t)i << 8) | (uint32_t)j;
+      acc[t] = 0;
+    }
+  }
+  __device__ __forceinline__ void add(const uint32_t (&gz)[LPT], const uint32_t (&gu)[LPT], int slot, int sub,
+                                      int lane, const ModP& M, const uint32_t (&)[3]) {
+#pragma unroll
+    for (int l = 0; l < LPT; ++l) {
+      zs[slot * B + LPT * sub + l] = gz[l];
+      us[slot * B + LPT * sub + l] = gu[l];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int t = 0; t < PPL; ++t) {
+      if (lane + 32 * t < NP) {
+        const int i = pij[t] >> 8, j = pij[t] & 0xff;
+        unsigned long long a = acc[t];
+#pragma unroll
+        for (int rr = 0; rr < RPW; ++rr) {
+          a = mad_wide(zs[rr * B + i], us[rr * B + j], a);
+          if ((rr % FE) == FE - 1) a = fold(a, M);
+        }
+        acc[t] = a;
+      }
+    }
+    __syncwarp();
+  }
+  __device__ __forceinline__ void finish(int, int, int, const ModP&, const uint32_t (&)[3]) {}
+  __device__ __forceinline__ void emit(unsigned long long* red, int lane, const ModP& M) {
+#pragma unroll
+    for (int t = 0; t < PPL; ++t) {
+      const int q = lane + 32 * t;
+      if (q < NP) atomicAdd(&red[q], (unsigned long long)reduce(acc[t], M));
+    }
+  }
+};
+
+// D += A * B with A 16x32 u8 (row-major fragments), B 32x8 u8, D 16x8 s32.
+__device__ __forceinline__ void mma_u8(int (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k32.row.col.s32.u8.u8.s32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+      : "+r"(d[0]), "+r"(d[1]), "+r"(d[2]), "+r"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// Tensor cores (B >= 8): exact integer Gram by byte limbs.  Residues are
+// < 2^31, so z = sum_a z_a 256^a with bytes z_a, and
+//   Z^T U = sum_{a,c} 256^{a+c} Z_a^T U_c.
+// A warp stages 32 rows (one K tile) as byte planes P[limb][lane][row] in
+// shared memory -- each row's four limbs are spread over four rows' words with
+// a 4x4 byte transpose across lanes (two shuffles and two byte permutes) --
+// then issues 16 m16n8k32 u8 MMAs per 16x8 output tile.  Per K tile a limb
+// pair's product is < 32 * 255^2 < 2^21, so the shift classes s = a + c stay
+// exact in int32; classes 0..3 are recombined exactly in 64 bits (< 2^48) and
+// classes 4..6 are added with their weights 2^{8s} mod p.
+template <int B, int FE>
+struct GramMma {
+  static constexpr int LPT = Shape<B>::LPT, TPR = Shape<B>::TPR, RPW = Shape<B>::RPW;
+  static constexpr int TB = 32 / RPW;           // batches per K tile
+  static constexpr int BM = B < 16 ? 16 : B;    // rows of the M dimension (zero padded)
+  static constexpr int MT = BM / 16, NT = B / 8;
+  static constexpr int RS = 9;                  // words per (limb, lane) plane row: 32 bytes + 4 pad
+  static constexpr int kPlane = 4 * BM * RS;    // words per plane set
+  static constexpr int kWords = 2 * kPlane;     // shared words per warp
+  uint32_t* pz;
+  uint32_t* pu;
+  unsigned long long acc[MT][NT][4];
+  int bt;
+
+  __device__ __forceinline__ void init(uint32_t* w, int lane) {
+    pz = w;
+    pu = w + kPlane;
+    for (int q = lane; q < kWords; q += 32) w[q] = 0;  // zero padding rows stay zero
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[mt][nt][v] = 0;
+    bt = 0;
+    __syncwarp();
+  }
+
+  // 4x4 byte transpose among the lanes holding rows 4q..4q+3 (lane distance
+  // TPR): afterwards byte k of the word of the lane with row 4q+rho is limb
+  // rho of the value of row 4q+k.
+  __device__ __forceinline__ static uint32_t transpose4(uint32_t w, int rho) {
+    uint32_t p = __shfl_xor_sync(0xffffffffu, w, TPR);
+    w = (rho & 1) ? __byte_perm(p, w, 0x7351) : __byte_perm(w, p, 0x6240);
+    p = __shfl_xor_sync(0xffffffffu, w, 2 * TPR);
+    return (rho & 2) ? __byte_perm(p, w, 0x7632) : __byte_perm(w, p, 0x5410);
+  }
+
+  __device__ __forceinline__ void stage(const uint32_t (&gz)[LPT], const uint32_t (&gu)[LPT], int slot, int sub) {
+    const int rho = slot & 3;
+    const int word = (bt * RPW + (slot & ~3)) >> 2;  // 4-row group inside the K tile
+#pragma unroll
+    for (int l = 0; l < LPT; ++l) {
+      const int i = LPT * sub + l;
+      pz[(rho * BM + i) * RS + word] = transpose4(gz[l], rho);
+      pu[(rho * BM + i) * RS + word] = transpose4(gu[l], rho);
+    }
+  }
+
+  __device__ __forceinline__ void flush(int lane, const ModP& M, const uint32_t (&W)[3]) {
+    __syncwarp();
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt) {
+      uint32_t A[4][4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        const uint32_t* r0 = pz + (a * BM + mt * 16 + g) * RS;
+        const uint32_t* r1 = r0 + 8 * RS;
+        A[a][0] = r0[t];
+        A[a][1] = r1[t];
+        A[a][2] = r0[t + 4];
+        A[a][3] = r1[t + 4];
+      }
+#pragma unroll
+      for (int nt = 0; nt < NT; ++nt) {
+        if (mt * 16 > nt * 8 + 7) continue;  // tile entirely below the diagonal
+        uint32_t Bf[4][2];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const uint32_t* r = pu + (c * BM + nt * 8 + g) * RS;
+          Bf[c][0] = r[t];
+          Bf[c][1] = r[t + 4];
+        }
+        uint64_t lo[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+          int C[4] = {0, 0, 0, 0};
+#pragma unroll
+          for (int a = 0; a <= s; ++a) mma_u8(C, A[a], Bf[s - a][0], Bf[s - a][1]);
+#pragma unroll
+          for (int v = 0; v < 4; ++v) lo[v] += (uint64_t)(uint32_t)C[v] << (8 * s);
+        }
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[mt][nt][v] = fold(acc[mt][nt][v] + lo[v], M);
+#pragma unroll
+        for (int s = 4; s < 7; ++s) {
+          int C[4] = {0, 0, 0, 0};
+#pragma unroll
+          for (int a = s - 3; a < 4; ++a) mma_u8(C, A[a], Bf[s - a][0], Bf[s - a][1]);
+#pragma unroll
+          for (int v = 0; v < 4; ++v) acc[mt][nt][v] = mad_wide((uint32_t)C[v], W[s - 4], acc[mt][nt][v]);
+        }
+      }
+    }
+    __syncwarp();
+  }
+
+  __device__ __forceinline__ void add(const uint32_t (&gz)[LPT], const uint32_t (&gu)[LPT], int slot, int sub,
+                                      int lane, const ModP& M, const uint32_t (&W)[3]) {
+    stage(gz, gu, slot, sub);
+    if (++bt == TB) {
+      flush(lane, M, W);
+      bt = 0;
+    }
+  }
+
+  __device__ __forceinline__ void finish(int slot, int sub, int lane, const ModP& M, const uint32_t (&W)[3]) {
+    if (bt == 0) return;
+    uint32_t z[LPT];
+#pragma unroll
+    for (int l = 0; l < LPT; ++l) z[l] = 0;
+    while (bt < TB) {  // zero the rows of the batches the tile did not get
+      stage(z, z, slot, sub);
+      ++bt;
+    }
+    flush(lane, M, W);
+    bt = 0;
+  }
+
+  __device__ __forceinline__ void emit(unsigned long long* red, int lane, const ModP& M) {
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          const int i = mt * 16 + g + (v >= 2 ? 8 : 0);
+          const int j = nt * 8 + 2 * t + (v & 1);
+          if (i <= j && j < B) atomicAdd(&red[pair_index(i, j, B)], (unsigned long long)reduce(acc[mt][nt][v], M));
+        }
+  }
+};
+
 template <int B, int MODE, int FE>
 __global__ void __launch_bounds__(kThreads) pass_kernel(PassParams P) {
-  constexpr int TPR = B / 4;          // threads per row (one uint4 each)
-  constexpr int RPW = 32 / TPR;       // rows per warp batch
-  constexpr int NP = B * (B + 1) / 2; // pairs in padded space
-  constexpr int PPL = (NP + 31) / 32; // pairs per lane
+  using S = Shape<B>;
+  constexpr int LPT = S::LPT, NV = S::NV, TPR = S::TPR, RPW = S::RPW;
+  constexpr int NP = B * (B + 1) / 2;  // pairs in padded space
+  constexpr bool kMma = B >= 8;
+  using Gram = typename std::conditional<kMma, GramMma<B, FE>, GramCore<B, FE>>::type;
 
-  __shared__ uint32_t zs[kWarps][RPW][B];
-  __shared__ uint32_t us[kWarps][RPW][B];
+  extern __shared__ __align__(16) uint32_t gram_smem[];
   __shared__ unsigned long long red[NP];
   __shared__ bool is_last;
 
@@ -95,19 +405,11 @@ __global__ void __launch_bounds__(kThreads) pass_kernel(PassParams P) {
   const int sub = lane % TPR;
   const int slot = lane / TPR;
   const ModP M = P.M;
+  const uint32_t W[3] = {P.w4, P.w5, P.w6};
 
   for (int q = threadIdx.x; q < NP; q += kThreads) red[q] = 0;
-
-  int pi[PPL], pj[PPL];
-#pragma unroll
-  for (int t = 0; t < PPL; ++t) {
-    const int q = lane + 32 * t;
-    if (q < NP) pair_of(q, B, pi[t], pj[t]);
-    else { pi[t] = 0; pj[t] = 0; }
-  }
-  unsigned long long gacc[PPL];
-#pragma unroll
-  for (int t = 0; t < PPL; ++t) gacc[t] = 0;
+  Gram gram;
+  if (P.S_out != nullptr) gram.init(gram_smem + (size_t)warp * Gram::kWords, lane);
 
   const int64_t nbatch = (P.rows + RPW - 1) / RPW;
   const int64_t gw = (int64_t)blockIdx.x * kWarps + warp;
@@ -115,109 +417,74 @@ __global__ void __launch_bounds__(kThreads) pass_kernel(PassParams P) {
 
   for (int64_t batch = gw; batch < nbatch; batch += nw) {
     const int64_t r = batch * RPW + slot;
-    uint32_t y[4] = {0, 0, 0, 0};
+    uint32_t gz[LPT], gu[LPT];
     if (r < P.rows) {
+      uint32_t t[LPT];
       if (MODE == kModeInit) {
-        const uint4 w = P.X[r * TPR + sub];
-        y[0] = w.x; y[1] = w.y; y[2] = w.z; y[3] = w.w;
-      } else if (r < P.heavy_rows) {
-        unsigned long long* h = P.heavy_acc + (size_t)r * B + 4 * sub;
 #pragma unroll
-        for (int l = 0; l < 4; ++l) {
-          y[l] = reduce(h[l], M);
-          h[l] = 0;
+        for (int v = 0; v < NV; ++v) {
+          const uint4 w = P.X[r * (B / 4) + sub * NV + v];
+          t[4 * v + 0] = w.x; t[4 * v + 1] = w.y; t[4 * v + 2] = w.z; t[4 * v + 3] = w.w;
         }
       } else {
-        const uint32_t beg = P.rowptr[r], end = P.rowptr[r + 1];
-        uint64_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-        uint32_t k = beg;
-        for (; k + FE <= end; k += FE) {
+        uint64_t acc[LPT];
 #pragma unroll
-          for (int u = 0; u < FE; ++u) {
-            const int32_t c = __ldg(P.col + k + u);
-            const uint32_t v = __ldg(P.val + k + u);
-            const uint4 x = __ldg(P.X + (size_t)c * TPR + sub);
-            a0 = mad_wide(v, x.x, a0);
-            a1 = mad_wide(v, x.y, a1);
-            a2 = mad_wide(v, x.z, a2);
-            a3 = mad_wide(v, x.w, a3);
+        for (int l = 0; l < LPT; ++l) acc[l] = 0;
+        if (r < P.heavy_rows) {
+          unsigned long long* h = P.heavy_acc + (size_t)r * B + LPT * sub;
+#pragma unroll
+          for (int l = 0; l < LPT; ++l) {
+            acc[l] = fold(h[l], M);
+            h[l] = 0;
           }
-          a0 = fold(a0, M); a1 = fold(a1, M); a2 = fold(a2, M); a3 = fold(a3, M);
+        } else {
+          gather_sum<B, FE>(P.cv, P.rowptr[r], P.rowptr[r + 1], 1u, P.X, sub, M, acc);
         }
-        for (; k < end; ++k) {
-          const int32_t c = __ldg(P.col + k);
-          const uint32_t v = __ldg(P.val + k);
-          const uint4 x = __ldg(P.X + (size_t)c * TPR + sub);
-          a0 = mad_wide(v, x.x, a0);
-          a1 = mad_wide(v, x.y, a1);
-          a2 = mad_wide(v, x.z, a2);
-          a3 = mad_wide(v, x.w, a3);
-        }
-        y[0] = reduce(a0, M); y[1] = reduce(a1, M); y[2] = reduce(a2, M); y[3] = reduce(a3, M);
+#pragma unroll
+        for (int l = 0; l < LPT; ++l) t[l] = redc(acc[l], M);  // t = (row sum) R^{-1}
       }
-    }
-    // epilogue: scale, store, stage the Gram operands
-    uint32_t gz[4], gu[4];
-    if (r < P.rows) {
-      const uint32_t s = P.scale[r];
-      uint4 o;
+      const uint32_t s1 = P.scale[r];
+      uint32_t o[LPT];
       if (MODE == kModeOdd) {
-        // z = y; U = d_r z
+        // z R^{-1} = t; U = d_r z = redc(t * d_r R^2)
 #pragma unroll
-        for (int l = 0; l < 4; ++l) { gz[l] = y[l]; gu[l] = mulmod(y[l], s, M); }
-        o = make_uint4(gu[0], gu[1], gu[2], gu[3]);
-      } else if (MODE == kModeEven) {
-        // w' = d_c t ; x' = d_c w'
-        uint32_t xo[4];
-#pragma unroll
-        for (int l = 0; l < 4; ++l) {
-          gz[l] = mulmod(y[l], s, M);
-          gu[l] = gz[l];
-          xo[l] = mulmod(gz[l], s, M);
+        for (int l = 0; l < LPT; ++l) {
+          gz[l] = t[l];
+          gu[l] = redc((uint64_t)t[l] * s1, M);
+          o[l] = gu[l];
         }
-        o = make_uint4(xo[0], xo[1], xo[2], xo[3]);
-      } else {
-        // init: y = w; x = d_c w
-        uint32_t xo[4];
+      } else if (MODE == kModeEven) {
+        // w' = d_c t_true = redc(t * d_c R^2); x' = d_c w' = redc(w' * d_c R)
+        const uint32_t s2 = P.scale2[r];
 #pragma unroll
-        for (int l = 0; l < 4; ++l) { gz[l] = y[l]; gu[l] = y[l]; xo[l] = mulmod(y[l], s, M); }
-        o = make_uint4(xo[0], xo[1], xo[2], xo[3]);
+        for (int l = 0; l < LPT; ++l) {
+          gz[l] = redc((uint64_t)t[l] * s1, M);
+          gu[l] = gz[l];
+          o[l] = redc((uint64_t)gz[l] * s2, M);
+        }
+      } else {
+        // init: w given; x = d_c w = redc(w * d_c R)
+#pragma unroll
+        for (int l = 0; l < LPT; ++l) {
+          gz[l] = t[l];
+          gu[l] = t[l];
+          o[l] = redc((uint64_t)t[l] * s1, M);
+        }
       }
-      P.Y[r * TPR + sub] = o;
+#pragma unroll
+      for (int v = 0; v < NV; ++v)
+        P.Y[r * (B / 4) + sub * NV + v] = make_uint4(o[4 * v], o[4 * v + 1], o[4 * v + 2], o[4 * v + 3]);
     } else {
 #pragma unroll
-      for (int l = 0; l < 4; ++l) { gz[l] = 0; gu[l] = 0; }
+      for (int l = 0; l < LPT; ++l) { gz[l] = 0; gu[l] = 0; }
     }
-    if (P.S_out != nullptr) {
-#pragma unroll
-      for (int l = 0; l < 4; ++l) {
-        zs[warp][slot][4 * sub + l] = gz[l];
-        us[warp][slot][4 * sub + l] = gu[l];
-      }
-      __syncwarp();
-#pragma unroll
-      for (int t = 0; t < PPL; ++t) {
-        if (lane + 32 * t < NP) {
-          unsigned long long a = gacc[t];
-#pragma unroll
-          for (int rr = 0; rr < RPW; ++rr) {
-            a = mad_wide(zs[warp][rr][pi[t]], us[warp][rr][pj[t]], a);
-            if ((rr % FE) == FE - 1) a = fold(a, M);
-          }
-          gacc[t] = a;
-        }
-      }
-      __syncwarp();
-    }
+    if (P.S_out != nullptr) gram.add(gz, gu, slot, sub, lane, M, W);
   }
 
   if (P.S_out == nullptr) return;
+  gram.finish(slot, sub, lane, M, W);
   __syncthreads();
-#pragma unroll
-  for (int t = 0; t < PPL; ++t) {
-    const int q = lane + 32 * t;
-    if (q < NP) atomicAdd(&red[q], (unsigned long long)reduce(gacc[t], M));
-  }
+  gram.emit(red, lane, M);
   __syncthreads();
   for (int q = threadIdx.x; q < NP; q += kThreads) atomicAdd(&P.gram_acc[q], red[q]);
   __threadfence();
@@ -233,20 +500,21 @@ __global__ void __launch_bounds__(kThreads) pass_kernel(PassParams P) {
     int i, j;
     pair_of(q, b, i, j);
     const int qb = i * B - i * (i - 1) / 2 + (j - i);
-    P.S_out[q] = reduce(atomicAdd(&P.gram_acc[qb], 0ull), M);
+    P.S_out[q] = mulmod(reduce(atomicAdd(&P.gram_acc[qb], 0ull), M), P.gram_mul, M);
   }
   __syncthreads();
   for (int q = threadIdx.x; q < NP; q += kThreads) atomicExch(&P.gram_acc[q], 0ull);
   if (threadIdx.x == 0) atomicExch(P.counter, 0u);
 }
 
-// Heavy rows: one warp per chunk of kChunkNnz entries.  Lanes form RPW slots
-// of TPR threads; slot s takes entries beg+s, beg+s+RPW, ...  The slot sums
-// are combined with shuffles and added to heavy_acc with 64-bit atomics.
+// Long rows: one warp per chunk of at most kChunkNnz entries.  Lanes form RPW
+// slots of TPR threads; slot s takes entries beg+s, beg+s+RPW, ...  The slot
+// sums (exact residues) are combined with shuffles and added to heavy_acc with
+// 64-bit atomics.
 template <int B, int FE>
 __global__ void __launch_bounds__(kThreads) chunk_kernel(ChunkParams P) {
-  constexpr int TPR = B / 4;
-  constexpr int RPW = 32 / TPR;
+  using S = Shape<B>;
+  constexpr int LPT = S::LPT, TPR = S::TPR, RPW = S::RPW;
   const int lane = threadIdx.x & 31;
   const int sub = lane % TPR;
   const int slot = lane / TPR;
@@ -256,41 +524,22 @@ __global__ void __launch_bounds__(kThreads) chunk_kernel(ChunkParams P) {
   for (int64_t ch = gw; ch < P.nchunks; ch += nw) {
     const uint32_t beg = P.chunk_begin[ch], end = P.chunk_end[ch];
     const uint32_t row = P.chunk_row[ch];
-    uint64_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-    uint32_t k = beg + slot;
-    for (; k + (FE - 1) * RPW < end; k += FE * RPW) {
+    uint64_t acc[LPT];
 #pragma unroll
-      for (int u = 0; u < FE; ++u) {
-        const uint32_t kk = k + u * RPW;
-        const int32_t c = __ldg(P.col + kk);
-        const uint32_t v = __ldg(P.val + kk);
-        const uint4 x = __ldg(P.X + (size_t)c * TPR + sub);
-        a0 = mad_wide(v, x.x, a0);
-        a1 = mad_wide(v, x.y, a1);
-        a2 = mad_wide(v, x.z, a2);
-        a3 = mad_wide(v, x.w, a3);
-      }
-      a0 = fold(a0, M); a1 = fold(a1, M); a2 = fold(a2, M); a3 = fold(a3, M);
-    }
-    for (; k < end; k += RPW) {
-      const int32_t c = __ldg(P.col + k);
-      const uint32_t v = __ldg(P.val + k);
-      const uint4 x = __ldg(P.X + (size_t)c * TPR + sub);
-      a0 = mad_wide(v, x.x, a0);
-      a1 = mad_wide(v, x.y, a1);
-      a2 = mad_wide(v, x.z, a2);
-      a3 = mad_wide(v, x.w, a3);
-    }
-    uint32_t y[4] = {reduce(a0, M), reduce(a1, M), reduce(a2, M), reduce(a3, M)};
+    for (int l = 0; l < LPT; ++l) acc[l] = 0;
+    gather_sum<B, FE>(P.cv, beg + slot, end, (uint32_t)RPW, P.X, sub, M, acc);
+    uint32_t y[LPT];
+#pragma unroll
+    for (int l = 0; l < LPT; ++l) y[l] = reduce(acc[l], M);
 #pragma unroll
     for (int off = TPR; off < 32; off <<= 1) {
 #pragma unroll
-      for (int l = 0; l < 4; ++l) y[l] = addmod(y[l], __shfl_xor_sync(0xffffffffu, y[l], off), M.p);
+      for (int l = 0; l < LPT; ++l) y[l] = addmod(y[l], __shfl_xor_sync(0xffffffffu, y[l], off), M.p);
     }
     if (slot == 0) {
-      unsigned long long* h = P.heavy_acc + (size_t)row * B + 4 * sub;
+      unsigned long long* h = P.heavy_acc + (size_t)row * B + LPT * sub;
 #pragma unroll
-      for (int l = 0; l < 4; ++l) atomicAdd(&h[l], (unsigned long long)y[l]);
+      for (int l = 0; l < LPT; ++l) atomicAdd(&h[l], (unsigned long long)y[l]);
     }
   }
 }
@@ -319,20 +568,36 @@ __global__ void gather_curv_kernel(const uint32_t* __restrict__ x, const uint32_
 }
 
 // ---------------------------------------------------------------- launchers
+// dynamic shared memory of the pass kernel: the per-warp Gram staging area
+template <int B>
+constexpr size_t pass_smem_bytes() {
+  return (size_t)kWarps * 4 * (B >= 8 ? GramMma<B, 4>::kWords : GramCore<B, 4>::kWords);
+}
+
 template <int B>
 static int launch_pass_B(rr_krylov* kr, const PassParams& P, int mode) {
   const dim3 grid(kr->grid_pass), block(kThreads);
   cudaStream_t s = kr->mat->ctx->stream;
+  const size_t sm = pass_smem_bytes<B>();
   if (kr->fold4) {
-    if (mode == kModeInit) pass_kernel<B, kModeInit, 4><<<grid, block, 0, s>>>(P);
-    else if (mode == kModeOdd) pass_kernel<B, kModeOdd, 4><<<grid, block, 0, s>>>(P);
-    else pass_kernel<B, kModeEven, 4><<<grid, block, 0, s>>>(P);
+    if (mode == kModeInit) pass_kernel<B, kModeInit, 4><<<grid, block, sm, s>>>(P);
+    else if (mode == kModeOdd) pass_kernel<B, kModeOdd, 4><<<grid, block, sm, s>>>(P);
+    else pass_kernel<B, kModeEven, 4><<<grid, block, sm, s>>>(P);
   } else {
-    if (mode == kModeInit) pass_kernel<B, kModeInit, 2><<<grid, block, 0, s>>>(P);
-    else if (mode == kModeOdd) pass_kernel<B, kModeOdd, 2><<<grid, block, 0, s>>>(P);
-    else pass_kernel<B, kModeEven, 2><<<grid, block, 0, s>>>(P);
+    if (mode == kModeInit) pass_kernel<B, kModeInit, 2><<<grid, block, sm, s>>>(P);
+    else if (mode == kModeOdd) pass_kernel<B, kModeOdd, 2><<<grid, block, sm, s>>>(P);
+    else pass_kernel<B, kModeEven, 2><<<grid, block, sm, s>>>(P);
   }
   RR_CUDA(cudaGetLastError());
+  return RR_OK;
+}
+
+template <int B, int FE>
+static int set_pass_smem() {
+  const int sm = (int)pass_smem_bytes<B>();
+  RR_CUDA(cudaFuncSetAttribute(pass_kernel<B, kModeInit, FE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  RR_CUDA(cudaFuncSetAttribute(pass_kernel<B, kModeOdd, FE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  RR_CUDA(cudaFuncSetAttribute(pass_kernel<B, kModeEven, FE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
   return RR_OK;
 }
 
@@ -370,11 +635,14 @@ static int launch_chunk(rr_krylov* kr, const ChunkParams& P) {
 
 template <int B>
 static int occupancy_B(rr_krylov* kr, int* pass_blocks, int* chunk_blocks) {
+  const size_t sm = pass_smem_bytes<B>();
   if (kr->fold4) {
-    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(pass_blocks, pass_kernel<B, kModeEven, 4>, kThreads, 0));
+    RR_TRY((set_pass_smem<B, 4>()));
+    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(pass_blocks, pass_kernel<B, kModeEven, 4>, kThreads, sm));
     RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(chunk_blocks, chunk_kernel<B, 4>, kThreads, 0));
   } else {
-    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(pass_blocks, pass_kernel<B, kModeEven, 2>, kThreads, 0));
+    RR_TRY((set_pass_smem<B, 2>()));
+    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(pass_blocks, pass_kernel<B, kModeEven, 2>, kThreads, sm));
     RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(chunk_blocks, chunk_kernel<B, 2>, kThreads, 0));
   }
   return RR_OK;
@@ -401,6 +669,10 @@ static PassParams base_params(rr_krylov* kr) {
   P.heavy_acc = kr->heavy_acc.ptr;
   P.gram_acc = kr->gram_acc.ptr;
   P.counter = kr->counter.ptr;
+  P.gram_mul = 1;
+  P.w4 = kr->M.c32;
+  P.w5 = (uint32_t)((uint64_t)kr->M.c32 * 256 % kr->M.p);
+  P.w6 = (uint32_t)((uint64_t)P.w5 * 256 % kr->M.p);
   P.b_real = kr->b;
   P.M = kr->M;
   return P;
@@ -413,7 +685,7 @@ int krylov_launch_init(rr_krylov* kr, const uint32_t* d_w, bool emit_s0) {
   P.heavy_rows = 0;
   P.X = reinterpret_cast<const uint4*>(d_w);
   P.Y = reinterpret_cast<uint4*>(kr->X[kr->cur].ptr);
-  P.scale = kr->dc.ptr;
+  P.scale = kr->dc_r.ptr;
   // S_0 goes to slot len - base; the caller publishes it (len += 1) later
   P.S_out = emit_s0 ? kr->S.ptr + (size_t)(kr->len - kr->base) * np : nullptr;
   return launch_pass(kr, P, kModeInit);
@@ -422,8 +694,7 @@ int krylov_launch_init(rr_krylov* kr, const uint32_t* d_w, bool emit_s0) {
 static int run_chunks(rr_krylov* kr, const DevCsr& A, const uint32_t* X) {
   if (A.nchunks == 0) return RR_OK;
   ChunkParams C;
-  C.col = A.col.ptr;
-  C.val = A.val.ptr;
+  C.cv = A.cv.ptr;
   C.chunk_row = A.chunk_row.ptr;
   C.chunk_begin = A.chunk_begin.ptr;
   C.chunk_end = A.chunk_end.ptr;
@@ -447,13 +718,13 @@ int krylov_launch_application(rr_krylov* kr, cudaEvent_t* ev) {
   RR_TRY(run_chunks(kr, mat->A, x));
   PassParams P = base_params(kr);
   P.rowptr = mat->A.rowptr.ptr;
-  P.col = mat->A.col.ptr;
-  P.val = mat->A.val.ptr;
+  P.cv = mat->A.cv.ptr;
   P.rows = mat->A.rows;
   P.heavy_rows = mat->A.heavy_rows;
   P.X = reinterpret_cast<const uint4*>(x);
   P.Y = reinterpret_cast<uint4*>(kr->U.ptr);
-  P.scale = kr->dr.ptr;
+  P.scale = kr->dr_m.ptr;
+  P.gram_mul = kr->M.r1;  // the odd Gram is accumulated from z R^{-1}
   P.S_out = kr->S.ptr + (size_t)(kr->len - kr->base) * np;
   RR_TRY(launch_pass(kr, P, kModeOdd));
   if (ev) RR_CUDA(cudaEventRecord(ev[1], s));
@@ -461,13 +732,14 @@ int krylov_launch_application(rr_krylov* kr, cudaEvent_t* ev) {
   RR_TRY(run_chunks(kr, mat->At, kr->U.ptr));
   if (ev) RR_CUDA(cudaEventRecord(ev[2], s));
   P.rowptr = mat->At.rowptr.ptr;
-  P.col = mat->At.col.ptr;
-  P.val = mat->At.val.ptr;
+  P.cv = mat->At.cv.ptr;
   P.rows = mat->At.rows;
   P.heavy_rows = mat->At.heavy_rows;
   P.X = reinterpret_cast<const uint4*>(kr->U.ptr);
   P.Y = reinterpret_cast<uint4*>(xn);
-  P.scale = kr->dc.ptr;
+  P.scale = kr->dc_m.ptr;
+  P.scale2 = kr->dc_r.ptr;
+  P.gram_mul = 1;
   P.S_out = kr->S.ptr + (size_t)(kr->len + 1 - kr->base) * np;
   RR_TRY(launch_pass(kr, P, kModeEven));
   if (ev) RR_CUDA(cudaEventRecord(ev[3], s));
@@ -501,13 +773,12 @@ int launch_scatter_block(rr_krylov* kr, const uint32_t* d_V, uint32_t* d_out) {
 // ---------------------------------------------------------------- matrix build
 // Host preprocessing: degree-ordered renumbering of rows and columns, the
 // transpose by counting sort (src/matrices.rs:734-778) and the chunk lists of
-// heavy rows; then one upload.
+// long rows; then one upload.
 namespace {
 
 struct HostCsr {
   std::vector<uint32_t> ptr;
-  std::vector<int32_t> col;
-  std::vector<uint32_t> val;
+  std::vector<uint2> cv;  // (column, value)
   int64_t rows = 0, cols = 0;
 };
 
@@ -522,32 +793,27 @@ void transpose_host(const HostCsr& a, HostCsr& t) {
   t.rows = a.cols;
   t.cols = a.rows;
   t.ptr.assign(a.cols + 1, 0);
-  for (int32_t c : a.col) t.ptr[c + 1]++;
+  for (const uint2& e : a.cv) t.ptr[e.x + 1]++;
   for (int64_t i = 0; i < a.cols; ++i) t.ptr[i + 1] += t.ptr[i];
   std::vector<uint32_t> next(t.ptr.begin(), t.ptr.end() - 1);
-  t.col.resize(a.col.size());
-  t.val.resize(a.val.size());
+  t.cv.resize(a.cv.size());
   for (int64_t r = 0; r < a.rows; ++r)
     for (uint32_t k = a.ptr[r]; k < a.ptr[r + 1]; ++k) {
-      const uint32_t pos = next[a.col[k]]++;
-      t.col[pos] = (int32_t)r;
-      t.val[pos] = a.val[k];
+      const uint32_t pos = next[a.cv[k].x]++;
+      t.cv[pos] = make_uint2((uint32_t)r, a.cv[k].y);
     }
 }
 
 int upload_csr(const HostCsr& h, DevCsr& d, cudaStream_t s) {
   d.rows = h.rows;
   d.cols = h.cols;
-  d.nnz = (int64_t)h.col.size();
+  d.nnz = (int64_t)h.cv.size();
   RR_TRY(d.rowptr.alloc(h.ptr.size()));
-  RR_TRY(d.col.alloc(std::max<size_t>(h.col.size(), 1)));
-  RR_TRY(d.val.alloc(std::max<size_t>(h.val.size(), 1)));
+  RR_TRY(d.cv.alloc(std::max<size_t>(h.cv.size(), 1)));
   RR_CUDA(cudaMemcpyAsync(d.rowptr.ptr, h.ptr.data(), h.ptr.size() * 4, cudaMemcpyHostToDevice, s));
-  if (!h.col.empty()) {
-    RR_CUDA(cudaMemcpyAsync(d.col.ptr, h.col.data(), h.col.size() * 4, cudaMemcpyHostToDevice, s));
-    RR_CUDA(cudaMemcpyAsync(d.val.ptr, h.val.data(), h.val.size() * 4, cudaMemcpyHostToDevice, s));
-  }
-  // heavy rows form a prefix (rows are sorted by decreasing degree)
+  if (!h.cv.empty())
+    RR_CUDA(cudaMemcpyAsync(d.cv.ptr, h.cv.data(), h.cv.size() * sizeof(uint2), cudaMemcpyHostToDevice, s));
+  // long rows form a prefix (rows are sorted by decreasing degree)
   int64_t heavy = 0;
   while (heavy < h.rows && (int64_t)(h.ptr[heavy + 1] - h.ptr[heavy]) > kHeavyDegree) ++heavy;
   d.heavy_rows = heavy;
@@ -556,7 +822,7 @@ int upload_csr(const HostCsr& h, DevCsr& d, cudaStream_t s) {
   for (int64_t r = 0; r < heavy; ++r)
     for (uint32_t k = h.ptr[r]; k < h.ptr[r + 1]; k += (uint32_t)kChunkNnz) {
       const uint32_t e = std::min<uint32_t>(h.ptr[r + 1], k + (uint32_t)kChunkNnz);
-      chunks.push_back({(uint32_t)r, k, e, (uint32_t)h.col[k]});
+      chunks.push_back({(uint32_t)r, k, e, h.cv[k].x});
     }
   // chunks that gather the same region of the input block run together
   std::stable_sort(chunks.begin(), chunks.end(), [](const Chunk& a, const Chunk& b) { return a.key < b.key; });
@@ -595,17 +861,13 @@ int matrix_build(rr_ctx* ctx, int64_t m, int64_t n, const int64_t* rowptr, const
   A.rows = m;
   A.cols = n;
   A.ptr.resize(m + 1);
-  A.col.resize(nnz);
-  A.val.resize(nnz);
+  A.cv.resize(nnz);
   A.ptr[0] = 0;
-  std::vector<std::pair<int32_t, uint32_t>> tmp;
   for (int64_t rp = 0; rp < m; ++rp) {
     const int64_t r = mat->rowperm[rp];
-    tmp.clear();
-    for (int64_t k = rowptr[r]; k < rowptr[r + 1]; ++k) tmp.push_back({inv_col[col[k]], val[k]});
-    std::sort(tmp.begin(), tmp.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
     uint32_t o = A.ptr[rp];
-    for (auto& e : tmp) { A.col[o] = e.first; A.val[o] = e.second; ++o; }
+    for (int64_t k = rowptr[r]; k < rowptr[r + 1]; ++k) A.cv[o++] = make_uint2((uint32_t)inv_col[col[k]], val[k]);
+    std::sort(A.cv.begin() + A.ptr[rp], A.cv.begin() + o, [](const uint2& a, const uint2& b) { return a.x < b.x; });
     A.ptr[rp + 1] = o;
   }
   HostCsr At;

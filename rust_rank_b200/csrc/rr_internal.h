@@ -78,15 +78,14 @@ namespace rr {
 // than kHeavyDegree entries and are processed by the chunk kernel.
 struct DevCsr {
   DevBuf<uint32_t> rowptr;  // rows + 1 offsets
-  DevBuf<int32_t> col;
-  DevBuf<uint32_t> val;
+  DevBuf<uint2> cv;         // packed (column, value) per entry
   int64_t rows = 0, cols = 0, nnz = 0;
   int64_t heavy_rows = 0;
   int64_t nchunks = 0;
   DevBuf<uint32_t> chunk_row, chunk_begin, chunk_end;
 };
 
-constexpr int64_t kHeavyDegree = 512;  // rows longer than this are split
+constexpr int64_t kHeavyDegree = 32;   // rows longer than this are split
 constexpr int64_t kChunkNnz = 1024;    // nonzeros per chunk of a split row
 
 }  // namespace rr
@@ -109,7 +108,9 @@ struct rr_krylov_s {
   int B = 0;   // padded width (4, 8, 16, 32)
   rr::ModP M{};
   int fold4 = 0;  // 1 when four products fit between folds
-  rr::DevBuf<uint32_t> dr, dc, dcinv;  // preconditioners in device order
+  // preconditioners in device order, in the forms the epilogues use:
+  // d_r R^2, d_c R^2, d_c R (mod p, R = 2^32) and d_c^{-1}
+  rr::DevBuf<uint32_t> dr_m, dc_m, dc_r, dcinv;
   rr::DevBuf<uint32_t> X[2];           // x_k = D_c w_k, n x B interleaved
   rr::DevBuf<uint32_t> U;              // D_r A x_k, m x B
   rr::DevBuf<unsigned long long> heavy_acc;

@@ -14,6 +14,8 @@ struct ModP {
   uint32_t p;      // the prime, p < 2^31
   uint32_t c32;    // 2^32 mod p
   uint64_t mu;     // floor(2^64 / p)
+  uint32_t pinv;   // -p^{-1} mod 2^32 (Montgomery reduction with R = 2^32)
+  uint32_t r1;     // R mod p
 };
 
 #ifdef __CUDACC__
@@ -30,6 +32,17 @@ __device__ __forceinline__ uint32_t reduce(uint64_t x, const ModP& M) {
   if (r >= M.p) r -= M.p;
   if (r >= M.p) r -= M.p;
   return (uint32_t)r;
+}
+
+// Montgomery reduction (Montgomery 1985), R = 2^32: for T < p * 2^32 returns
+// T * R^{-1} mod p in [0, p).  m = T * (-p^{-1}) mod R makes T + m p divisible
+// by R, and T + m p < 2 p R < 2^64.  A folded accumulator always satisfies
+// the bound, since fold() < (2^32 - 1) * c32 + 2^32 <= (2^32 - 1) * p + 2^32 - 1.
+__device__ __forceinline__ uint32_t redc(uint64_t T, const ModP& M) {
+  const uint32_t m = (uint32_t)T * M.pinv;
+  const uint64_t s = (uint64_t)m * M.p + T;
+  const uint32_t t = (uint32_t)(s >> 32);
+  return t >= M.p ? t - M.p : t;
 }
 
 __device__ __forceinline__ uint32_t mulmod(uint32_t a, uint32_t b, const ModP& M) {
