@@ -389,7 +389,9 @@ struct GramMma {
 };
 
 template <int B, int MODE, int FE>
-__global__ void __launch_bounds__(kThreads) pass_kernel(PassParams P) {
+// Four CTAs (32 warps) per SM: the walk is latency bound, so occupancy is
+// worth a few spilled registers (measured on the 2M x 1.5M Zipf matrix).
+__global__ void __launch_bounds__(kThreads, 4) pass_kernel(PassParams P) {
   using S = Shape<B>;
   constexpr int LPT = S::LPT, NV = S::NV, TPR = S::TPR, RPW = S::RPW;
   constexpr int NP = B * (B + 1) / 2;  // pairs in padded space
@@ -512,7 +514,7 @@ __global__ void __launch_bounds__(kThreads) pass_kernel(PassParams P) {
 // sums (exact residues) are combined with shuffles and added to heavy_acc with
 // 64-bit atomics.
 template <int B, int FE>
-__global__ void __launch_bounds__(kThreads) chunk_kernel(ChunkParams P) {
+__global__ void __launch_bounds__(kThreads, 3) chunk_kernel(ChunkParams P) {
   using S = Shape<B>;
   constexpr int LPT = S::LPT, TPR = S::TPR, RPW = S::RPW;
   const int lane = threadIdx.x & 31;
