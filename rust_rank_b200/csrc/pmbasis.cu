@@ -43,7 +43,8 @@ namespace rr {
 namespace {
 
 constexpr int kNttBlock = 4096;  // elements transformed per CTA in shared memory
-constexpr int kBaseThreads = 256;
+constexpr int kBaseThreads = 512;
+constexpr size_t kBaseSmemBudget = 220 * 1024;  // dynamic shared memory of one block kernel
 
 struct Twiddles {
   const uint32_t* w;   // omega^j, j < Nmax/2
@@ -254,7 +255,8 @@ struct BaseParams {
   int64_t* delta;      // [m], in/out
   uint32_t* Mout;      // Mout[i][j][t], row stride out_rs, column stride out_cs, t <= nleaves
   int64_t out_rs, out_cs;
-  uint32_t* Mbuf;      // scratch: 2 x (nleaves+1) x m x m
+  uint32_t* Mbuf;      // scratch: 2 x (nleaves+1) x m x m, used unless m_smem
+  int m_smem;          // keep the block's basis in shared memory
   ModP M;
   int* status;
 };
@@ -271,6 +273,13 @@ __device__ uint32_t inv_fermat(uint32_t a, const ModP& M) {
 }
 
 // One CTA runs nleaves order-1 leaves on G's first nleaves coefficients.
+// VEC = 4 when 4 | b: the residual and basis updates then compute four
+// adjacent columns per thread from 128-bit shared-memory reads.
+// Arithmetic: every elimination and update ends in a Montgomery reduction, so
+// each leaf multiplies the rows of the residual and of the basis by a known
+// non-zero factor (c_i R^{-1}); sigma tracks it and the block's basis is
+// normalised once at the end.
+template <int VEC>
 __global__ void __launch_bounds__(kBaseThreads) pm_base_kernel(BaseParams P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int m = P.m, n = P.n, K = P.nleaves;
@@ -279,7 +288,8 @@ __global__ void __launch_bounds__(kBaseThreads) pm_base_kernel(BaseParams P) {
   const uint32_t p = M.p;
   uint32_t* R0 = reinterpret_cast<uint32_t*>(smem_raw);
   uint32_t* R1 = R0 + (size_t)K * m * n;
-  uint32_t* A = R1 + (size_t)K * m * n;  // m x W
+  uint32_t* MS = R1 + (size_t)K * m * n;                     // basis in shared memory (2 x (K+1) x m x m) or empty
+  uint32_t* A = MS + (P.m_smem ? (size_t)2 * (K + 1) * m * m : 0);  // m x W
   uint32_t* T = A + (size_t)m * W;      // m x m
   uint32_t* fcol = T + (size_t)m * m;   // m
   uint32_t* sigma = fcol + m;           // m
@@ -302,8 +312,8 @@ __global__ void __launch_bounds__(kBaseThreads) pm_base_kernel(BaseParams P) {
     sdelta[i] = P.delta[i];
     sigma[i] = 1;
   }
-  uint32_t* Mc = P.Mbuf;                              // current basis [t][i][j]
-  uint32_t* Mn = P.Mbuf + (size_t)(K + 1) * m * m;    // next basis
+  uint32_t* Mc = P.m_smem ? MS : P.Mbuf;                            // current basis [t][i][j]
+  uint32_t* Mn = Mc + (size_t)(K + 1) * m * m;                      // next basis
   for (int e = tid; e < m * m; e += nt) Mc[e] = (e / m == e % m) ? 1u : 0u;
   __syncthreads();
 
@@ -371,20 +381,21 @@ __global__ void __launch_bounds__(kBaseThreads) pm_base_kernel(BaseParams P) {
         const int rows = m - k - 1;
         for (int e = tid; e < rows * W; e += nt) {
           const int i = k + 1 + e / W, c = e % W;
-          // piv * a_ic - a_ic* * a_kc  (exact, then one reduction)
+          // (piv * a_ic - a_ic* * a_kc) R^{-1}: the row keeps a non-zero scale
           const uint64_t acc = mad_wide(piv, A[(size_t)i * W + c], (uint64_t)(p - fcol[i]) * ak[c]);
-          A[(size_t)i * W + c] = reduce(acc, M);
+          A[(size_t)i * W + c] = redc(acc, M);
         }
       }
       // no warp may rewrite the step flags before every warp has read them
       __syncthreads();
     }
-    // T = scaled L^{-1} pi; c_i = T[i][perm[i]]; sigma_new[i] = c_i sigma[perm[i]]
+    // T = scaled L^{-1} pi; c_i = T[i][perm[i]]; rows of the updates below are
+    // multiplied by c_i R^{-1}
     for (int e = tid; e < m * m; e += nt) T[e] = A[(size_t)(e / m) * W + n + (e % m)];
     for (int i = tid; i < m; i += nt) {
       const uint32_t ci = A[(size_t)i * W + n + perm[i]];
       if (ci == 0) atomicExch(P.status, 2);
-      sig_tmp[i] = mulmod(ci, sigma[perm[i]], M);
+      sig_tmp[i] = redc((uint64_t)ci * sigma[perm[i]], M);
       sdelta_tmp[i] = sdelta[perm[i]] - mask[i];  // src/sigma_basis.rs:408-411
     }
     __syncthreads();
@@ -394,39 +405,68 @@ __global__ void __launch_bounds__(kBaseThreads) pm_base_kernel(BaseParams P) {
     }
     // residual: Rn[t][i] = T_i . Rc[t + 1 - mask_i], t < K - leaf - 1
     const int rem = K - leaf - 1;
-    for (int e = tid; e < rem * m * n; e += nt) {
-      const int t = e / (m * n), i = (e / n) % m, c = e % n;
+    const int nq = n / VEC;
+    for (int e = tid; e < rem * m * nq; e += nt) {
+      const int t = e / (m * nq), i = (e / nq) % m, c = (e % nq) * VEC;
       const uint32_t* src = Rc + (size_t)(t + 1 - mask[i]) * m * n + c;
       const uint32_t* ti = T + (size_t)i * m;
-      uint64_t acc = 0;
-      int s = 0;
-      for (; s + 1 < m; s += 2) {
-        acc = mad_wide(ti[s], src[(size_t)s * n], acc);
-        acc = mad_wide(ti[s + 1], src[(size_t)(s + 1) * n], acc);
-        acc = fold(acc, M);
+      uint64_t acc[VEC];
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) acc[v] = 0;
+      for (int s = 0; s < m; ++s) {
+        const uint32_t w = ti[s];
+        if (VEC == 4) {
+          const uint4 x = *reinterpret_cast<const uint4*>(src + (size_t)s * n);
+          acc[0] = mad_wide(w, x.x, acc[0]);
+          acc[VEC > 1 ? 1 : 0] = mad_wide(w, x.y, acc[VEC > 1 ? 1 : 0]);
+          acc[VEC > 2 ? 2 : 0] = mad_wide(w, x.z, acc[VEC > 2 ? 2 : 0]);
+          acc[VEC > 3 ? 3 : 0] = mad_wide(w, x.w, acc[VEC > 3 ? 3 : 0]);
+        } else {
+          acc[0] = mad_wide(w, src[(size_t)s * n], acc[0]);
+        }
+        if (s & 1) {
+#pragma unroll
+          for (int v = 0; v < VEC; ++v) acc[v] = fold(acc[v], M);
+        }
       }
-      if (s < m) acc = mad_wide(ti[s], src[(size_t)s * n], acc);
-      Rn[e] = reduce(acc, M);
+      uint32_t* dst = Rn + (size_t)t * m * n + (size_t)i * n + c;
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) dst[v] = redc(fold(acc[v], M), M);
     }
     // basis: Mn[t][i] = T_i . Mc[t - mask_i], t <= leaf + 1
-    for (int e = tid; e < (leaf + 2) * m * m; e += nt) {
-      const int t = e / (m * m), i = (e / m) % m, c = e % m;
+    const int mq = m / VEC;
+    for (int e = tid; e < (leaf + 2) * m * mq; e += nt) {
+      const int t = e / (m * mq), i = (e / mq) % m, c = (e % mq) * VEC;
       const int st = t - mask[i];
-      uint32_t out = 0;
-      if (st >= 0 && st <= leaf) {
-        const uint32_t* src = Mc + (size_t)st * m * m + c;
-        const uint32_t* ti = T + (size_t)i * m;
-        uint64_t acc = 0;
-        int s = 0;
-        for (; s + 1 < m; s += 2) {
-          acc = mad_wide(ti[s], src[(size_t)s * m], acc);
-          acc = mad_wide(ti[s + 1], src[(size_t)(s + 1) * m], acc);
-          acc = fold(acc, M);
-        }
-        if (s < m) acc = mad_wide(ti[s], src[(size_t)s * m], acc);
-        out = reduce(acc, M);
+      uint32_t* dst = Mn + (size_t)t * m * m + (size_t)i * m + c;
+      if (st < 0 || st > leaf) {
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) dst[v] = 0;
+        continue;
       }
-      Mn[e] = out;
+      const uint32_t* src = Mc + (size_t)st * m * m + c;
+      const uint32_t* ti = T + (size_t)i * m;
+      uint64_t acc[VEC];
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) acc[v] = 0;
+      for (int s = 0; s < m; ++s) {
+        const uint32_t w = ti[s];
+        if (VEC == 4) {
+          const uint4 x = *reinterpret_cast<const uint4*>(src + (size_t)s * m);
+          acc[0] = mad_wide(w, x.x, acc[0]);
+          acc[VEC > 1 ? 1 : 0] = mad_wide(w, x.y, acc[VEC > 1 ? 1 : 0]);
+          acc[VEC > 2 ? 2 : 0] = mad_wide(w, x.z, acc[VEC > 2 ? 2 : 0]);
+          acc[VEC > 3 ? 3 : 0] = mad_wide(w, x.w, acc[VEC > 3 ? 3 : 0]);
+        } else {
+          acc[0] = mad_wide(w, src[(size_t)s * m], acc[0]);
+        }
+        if (s & 1) {
+#pragma unroll
+          for (int v = 0; v < VEC; ++v) acc[v] = fold(acc[v], M);
+        }
+      }
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) dst[v] = redc(fold(acc[v], M), M);
     }
     __syncthreads();
     uint32_t* tr = Rc; Rc = Rn; Rn = tr;
@@ -440,6 +480,15 @@ __global__ void __launch_bounds__(kBaseThreads) pm_base_kernel(BaseParams P) {
     const int t = e / (m * m), i = (e / m) % m, c = e % m;
     P.Mout[(int64_t)i * P.out_rs + (int64_t)c * P.out_cs + t] = mulmod(Mc[e], sig_tmp[i], M);
   }
+}
+
+// Shared-memory bytes of pm_base_kernel for m rows, n columns, K leaves.
+size_t base_smem_bytes(int m, int n, int K, bool m_smem) {
+  size_t words = (size_t)2 * K * m * n + (m_smem ? (size_t)2 * (K + 1) * m * m : 0) + (size_t)m * (n + m) +
+                 (size_t)m * m + 3 * (size_t)m + 1;
+  size_t bytes = (words * 4 + 7) & ~(size_t)7;
+  bytes += 2 * (size_t)m * 8 + 3 * (size_t)m * 4 + 64;
+  return bytes;
 }
 
 // ---------------------------------------------------------------- host side
@@ -567,10 +616,27 @@ int run_base(Pm& P, const uint32_t* G, int64_t g_rs, int64_t g_cs, int nleaves, 
   B.out_rs = o_rs;
   B.out_cs = o_cs;
   B.Mbuf = P.Mbuf.ptr;
+  B.m_smem = 1;
   B.M = P.M;
   B.status = P.status.ptr;
-  pm_base_kernel<<<1, kBaseThreads, P.base_smem, P.s>>>(B);
+  if (P.n % 4 == 0) pm_base_kernel<4><<<1, kBaseThreads, P.base_smem, P.s>>>(B);
+  else pm_base_kernel<1><<<1, kBaseThreads, P.base_smem, P.s>>>(B);
   RR_CUDA(cudaGetLastError());
+  return RR_OK;
+}
+
+// Largest block of leaves (a power of two <= 32 and <= d) whose residual and
+// basis fit in shared memory.
+int pick_block_leaves(int m, int n, int64_t d, size_t* smem) {
+  int K = (int)std::min<int64_t>(d, 32);
+  while (K > 1 && base_smem_bytes(m, n, K, true) > kBaseSmemBudget) K /= 2;
+  *smem = base_smem_bytes(m, n, K, true);
+  return K;
+}
+
+int set_base_smem_limit(size_t bytes) {
+  RR_CUDA(cudaFuncSetAttribute(pm_base_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  RR_CUDA(cudaFuncSetAttribute(pm_base_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
   return RR_OK;
 }
 
@@ -604,7 +670,7 @@ int pm_basis_device(rr_ctx* ctx, const uint32_t* seq, int64_t seq_stride, int b,
   P.n = b;
   P.p = p;
   P.M = make_modp(p);
-  P.K = (int)std::min<int64_t>(d, P.m <= 32 ? 32 : 8);
+  P.K = pick_block_leaves(P.m, P.n, d, &P.base_smem);
   const int m = P.m, n = P.n;
   // NTT table for the largest product: length nextpow2(3d/2 + 1) = 2d (d >= 2)
   int64_t nmax = 1;
@@ -652,20 +718,11 @@ int pm_basis_device(rr_ctx* ctx, const uint32_t* seq, int64_t seq_stride, int b,
       }
     }
   }
-  RR_TRY(P.Mbuf.alloc((size_t)2 * (P.K + 1) * m * m));
   RR_TRY(P.delta.alloc(m));
   RR_TRY(P.status.alloc(1));
   RR_CUDA(cudaMemsetAsync(P.delta.ptr, 0, m * sizeof(int64_t), P.s));
   RR_CUDA(cudaMemsetAsync(P.status.ptr, 0, sizeof(int), P.s));
-  {
-    const int K = P.K;
-    size_t words = (size_t)2 * K * m * n + (size_t)m * (n + m) + (size_t)m * m + 3 * (size_t)m + 1;
-    size_t bytes = words * 4;
-    bytes = (bytes + 7) & ~(size_t)7;
-    bytes += 2 * (size_t)m * 8 + 3 * (size_t)m * 4 + 64;
-    P.base_smem = bytes;
-    RR_CUDA(cudaFuncSetAttribute(pm_base_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-  }
+  RR_TRY(set_base_smem_limit(P.base_smem));
   // G = [S; I], coefficients [0, d]
   DevBuf<uint32_t> dseq, G;
   const int np = b * (b + 1) / 2;
@@ -771,14 +828,13 @@ extern "C" int rr_pm_basis_short_noalloc(const uint32_t* d_seq, int64_t seq_stri
   B.out_rs = (int64_t)m * glen;
   B.out_cs = glen;
   B.Mbuf = Mbuf;
+  B.m_smem = 0;  // the basis stays in the scratch array
   B.M = make_modp(p);
   B.status = status;
-  const int K = (int)dd;
-  size_t words = (size_t)2 * K * m * n + (size_t)m * (n + m) + (size_t)m * m + 3 * (size_t)m + 1;
-  size_t bytes = (words * 4 + 7) & ~(size_t)7;
-  bytes += 2 * (size_t)m * 8 + 3 * (size_t)m * 4 + 64;
-  RR_CUDA(cudaFuncSetAttribute(pm_base_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-  pm_base_kernel<<<1, kBaseThreads, bytes, s>>>(B);
+  const size_t bytes = base_smem_bytes(m, n, (int)dd, false);
+  RR_TRY(set_base_smem_limit(bytes));
+  if (n % 4 == 0) pm_base_kernel<4><<<1, kBaseThreads, bytes, s>>>(B);
+  else pm_base_kernel<1><<<1, kBaseThreads, bytes, s>>>(B);
   RR_CUDA(cudaGetLastError());
   return RR_OK;
 }
