@@ -38,6 +38,7 @@ typedef enum rr_status {
 typedef struct rr_ctx_s rr_ctx;       /* one device + one CUDA stream */
 typedef struct rr_matrix_s rr_matrix; /* a sparse matrix resident on the device */
 typedef struct rr_krylov_s rr_krylov; /* Krylov state of one block of vectors */
+typedef struct rr_batch_s rr_batch;   /* many matrices stacked for one Krylov launch per pass */
 
 const char* rr_status_string(int status);
 /* Message of the last failed call on this thread ("" if none). */
@@ -155,6 +156,33 @@ int rr_rank_from_basis(const uint32_t* M, const int64_t* delta, int32_t b, int64
  * d = largest power of two <= length, rank readout. */
 int rr_rank(rr_matrix* mat, int32_t b, const uint32_t* row_precond, const uint32_t* col_precond,
             const uint32_t* V, int64_t max_nlen, int64_t* rank);
+
+/* ---------------------------------------------------------------- batches */
+/* Many matrices (one per degree of a graph complex; the reference runs them
+ * one main.rs invocation each, commands.txt) ranked together.  Matrix i is
+ * m[i] x n[i] CSR (rowptr[i][m[i]+1], col[i], val[i] reduced mod p) with its
+ * preconditioners and V[i] ([b][n[i]]).  Every matrix gets the sequence
+ * length rule of src/main.rs:497-504 and the same sequence, generator and
+ * rank as rr_rank on it alone.  The batch is copied at create time. */
+int rr_batch_create(rr_ctx* ctx, int32_t nmat, const int64_t* m, const int64_t* n, const int64_t* const* rowptr,
+                    const int32_t* const* col, const uint32_t* const* val, uint32_t p, int32_t b,
+                    const uint32_t* const* row_precond, const uint32_t* const* col_precond,
+                    const uint32_t* const* V, rr_batch** out);
+int rr_batch_destroy(rr_batch* batch);
+/* All Krylov sequences: S_0 for every matrix, then one launch per pass of B
+ * over the matrices whose sequences are still running.  Once per batch. */
+int rr_batch_krylov(rr_batch* batch);
+/* Sequence of matrix i: *len = its length; seq [b(b+1)/2][seq_stride >= len]
+ * (src/main.rs:164-175 order), or NULL to query the length only. */
+int rr_batch_sequence(rr_batch* batch, int32_t i, uint32_t* seq, int64_t seq_stride, int64_t* len);
+/* Generators and ranks of all matrices (runs rr_batch_krylov first when it
+ * has not run), `workers` generators in flight on streams of their own.
+ * ranks[nmat] in the caller's order; RR_ESTATE as rr_rank_from_basis. */
+int rr_batch_ranks(rr_batch* batch, int32_t workers, int64_t* ranks);
+/* Stacked sizes: rows and columns with padding, nonzeros, applications of
+ * B of the longest sequence. */
+int rr_batch_info(const rr_batch* batch, int64_t* total_rows, int64_t* total_cols, int64_t* total_nnz,
+                  int64_t* max_apps);
 
 /* ---------------------------------------------------------------- files */
 /* .wdm checkpoint (src/wdm_files.rs:10-19): header "m n p Nlen num_v", then

@@ -297,6 +297,71 @@ def block_wiedemann_rank(a: CsrMatrix | DeviceMatrix, num_v: int, theprime: int 
     return r.value
 
 
+class Batch:
+    """Many matrices ranked together (rr_batch_*): one Krylov launch per pass
+    for the whole stack, generators solved concurrently as sequences finish.
+
+    ``mats`` is a list of (rowptr, col, val, m, n); ``row_preconds``,
+    ``col_preconds`` and ``vs`` give each matrix's preconditioners and its
+    b x n block V.  Every matrix gets the same sequence, generator and rank
+    as :func:`block_wiedemann_rank` on it alone."""
+
+    def __init__(self, mats, num_v: int, theprime: int, row_preconds, col_preconds, vs, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        self.n = len(mats)
+        self.b = int(num_v)
+        keep = []
+
+        def arr(xs, dt):
+            out = [np.ascontiguousarray(x, dt) for x in xs]
+            keep.extend(out)
+            return (C.c_void_p * self.n)(*[a.ctypes.data for a in out])
+
+        m = np.array([int(x[3]) for x in mats], np.int64)
+        n = np.array([int(x[4]) for x in mats], np.int64)
+        rp = arr([x[0] for x in mats], np.int64)
+        cl = arr([x[1] for x in mats], np.int32)
+        vl = arr([x[2] for x in mats], np.uint32)
+        rpc = arr(row_preconds, np.uint32)
+        cpc = arr(col_preconds, np.uint32)
+        vv = arr(vs, np.uint32)
+        h = C.c_void_p()
+        check(lib().rr_batch_create(self.ctx.handle, self.n, ptr(m), ptr(n), rp, cl, vl, int(theprime), self.b, rpc,
+                                    cpc, vv, C.byref(h)))
+        self.handle = h
+
+    def krylov(self):
+        check(lib().rr_batch_krylov(self.handle))
+
+    def sequence(self, i: int) -> np.ndarray:
+        L = C.c_int64()
+        check(lib().rr_batch_sequence(self.handle, i, None, 0, C.byref(L)))
+        seq = np.zeros((self.b * (self.b + 1) // 2, L.value), np.uint32)
+        check(lib().rr_batch_sequence(self.handle, i, ptr(seq), L.value, C.byref(L)))
+        return seq
+
+    def ranks(self, workers: int = 8) -> np.ndarray:
+        out = np.zeros(self.n, np.int64)
+        check(lib().rr_batch_ranks(self.handle, int(workers), ptr(out)))
+        return out
+
+    def info(self):
+        r, c, z, a = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()
+        check(lib().rr_batch_info(self.handle, C.byref(r), C.byref(c), C.byref(z), C.byref(a)))
+        return {"rows": r.value, "cols": c.value, "nnz": z.value, "max_apps": a.value}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().rr_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def save_wdm_file_sym(path: str, n_rows: int, n_cols: int, theprime: int, row_precond, col_precond, v, curv, seq):
     """src/wdm_files.rs:126-210."""
     v = np.ascontiguousarray(v, np.uint32)

@@ -37,41 +37,9 @@
 #include <numeric>
 #include <type_traits>
 
-#include "rr_internal.h"
+#include "krylov_params.h"
 
 namespace rr {
-
-enum PassMode { kModeInit = 0, kModeOdd = 1, kModeEven = 2 };
-
-struct PassParams {
-  const uint32_t* rowptr;
-  const uint2* cv;          // packed (column, value)
-  int64_t rows;
-  int64_t heavy_rows;
-  const uint4* X;           // gathered block [cols][B/4]   (kModeInit: w [rows][B/4])
-  uint4* Y;                 // output block   [rows][B/4]
-  const uint32_t* scale;    // odd: d_r R^2; even: d_c R^2; init: d_c R   (all mod p)
-  const uint32_t* scale2;   // even: d_c R
-  unsigned long long* heavy_acc;  // [heavy_rows][B]
-  unsigned long long* gram_acc;   // [B(B+1)/2]
-  unsigned int* counter;
-  uint32_t* S_out;          // finished term, real pairs; nullptr = do not emit
-  uint32_t gram_mul;        // factor applied to the finished term
-  uint32_t w4, w5, w6;      // 2^32, 2^40, 2^48 mod p (limb weights of the tensor-core Gram)
-  int b_real;
-  ModP M;
-};
-
-struct ChunkParams {
-  const uint2* cv;
-  const uint32_t* chunk_row;
-  const uint32_t* chunk_begin;
-  const uint32_t* chunk_end;
-  int64_t nchunks;
-  const uint4* X;
-  unsigned long long* heavy_acc;
-  ModP M;
-};
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
@@ -226,6 +194,10 @@ struct GramCore {
     __syncwarp();
   }
   __device__ __forceinline__ void finish(int, int, int, const ModP&, const uint32_t (&)[3]) {}
+  __device__ __forceinline__ void reset() {
+#pragma unroll
+    for (int t = 0; t < PPL; ++t) acc[t] = 0;
+  }
   __device__ __forceinline__ void emit(unsigned long long* red, int lane, const ModP& M) {
 #pragma unroll
     for (int t = 0; t < PPL; ++t) {
@@ -360,6 +332,16 @@ struct GramMma {
     }
   }
 
+  __device__ __forceinline__ void reset() {
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[mt][nt][v] = 0;
+    bt = 0;
+  }
+
   __device__ __forceinline__ void finish(int slot, int sub, int lane, const ModP& M, const uint32_t (&W)[3]) {
     if (bt == 0) return;
     uint32_t z[LPT];
@@ -416,8 +398,31 @@ __global__ void __launch_bounds__(kThreads, 4) pass_kernel(PassParams P) {
   const int64_t nbatch = (P.rows + RPW - 1) / RPW;
   const int64_t gw = (int64_t)blockIdx.x * kWarps + warp;
   const int64_t nw = (int64_t)gridDim.x * kWarps;
+  const bool segmented = P.batch_seg != nullptr;
+  // one matrix: grid-stride over the degree-sorted batches; batched: contiguous
+  // runs, so that a warp changes matrix (and flushes its Gram terms) rarely
+  int64_t b_first = gw, b_stop = nbatch, b_step = nw;
+  if (segmented) {
+    const int64_t total = nbatch - P.batch_begin;
+    const int64_t q = (total + nw - 1) / nw;
+    b_first = P.batch_begin + gw * q;
+    b_stop = b_first + q < nbatch ? b_first + q : nbatch;
+    b_step = 1;
+  }
+  int cur_seg = -1;
 
-  for (int64_t batch = gw; batch < nbatch; batch += nw) {
+  for (int64_t batch = b_first; batch < b_stop; batch += b_step) {
+    if (segmented && P.S_out != nullptr) {
+      const int sg = P.batch_seg[batch];
+      if (sg != cur_seg) {
+        if (cur_seg >= 0) {
+          gram.finish(slot, sub, lane, M, W);
+          gram.emit(P.gram_acc + (size_t)cur_seg * NP, lane, M);
+          gram.reset();
+        }
+        cur_seg = sg;
+      }
+    }
     const int64_t r = batch * RPW + slot;
     uint32_t gz[LPT], gu[LPT];
     if (r < P.rows) {
@@ -485,27 +490,42 @@ __global__ void __launch_bounds__(kThreads, 4) pass_kernel(PassParams P) {
 
   if (P.S_out == nullptr) return;
   gram.finish(slot, sub, lane, M, W);
-  __syncthreads();
-  gram.emit(red, lane, M);
-  __syncthreads();
-  for (int q = threadIdx.x; q < NP; q += kThreads) atomicAdd(&P.gram_acc[q], red[q]);
+  if (segmented) {
+    if (cur_seg >= 0) gram.emit(P.gram_acc + (size_t)cur_seg * NP, lane, M);
+  } else {
+    __syncthreads();
+    gram.emit(red, lane, M);
+    __syncthreads();
+    for (int q = threadIdx.x; q < NP; q += kThreads) atomicAdd(&P.gram_acc[q], red[q]);
+  }
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) is_last = (atomicAdd(P.counter, 1u) == gridDim.x - 1);
   __syncthreads();
   if (!is_last) return;
   __threadfence();
-  // the last CTA: write the finished term (real pairs only) and reset
+  // the last CTA: write the finished terms (real pairs only) and reset
   const int b = P.b_real;
   const int npr = b * (b + 1) / 2;
-  for (int q = threadIdx.x; q < npr; q += kThreads) {
-    int i, j;
-    pair_of(q, b, i, j);
-    const int qb = i * B - i * (i - 1) / 2 + (j - i);
-    P.S_out[q] = mulmod(reduce(atomicAdd(&P.gram_acc[qb], 0ull), M), P.gram_mul, M);
+  if (segmented) {
+    const int nseg = P.seg_end - P.seg_begin;
+    for (int64_t e = threadIdx.x; e < (int64_t)nseg * npr; e += kThreads) {
+      const int s = P.seg_begin + (int)(e / npr), q = (int)(e % npr);
+      int i, j;
+      pair_of(q, b, i, j);
+      unsigned long long* g = P.gram_acc + (size_t)s * NP + pair_index(i, j, B);
+      P.S_all[P.seg_S_off[s] + P.term * npr + q] = mulmod(reduce(atomicExch(g, 0ull), M), P.gram_mul, M);
+    }
+  } else {
+    for (int q = threadIdx.x; q < npr; q += kThreads) {
+      int i, j;
+      pair_of(q, b, i, j);
+      const int qb = i * B - i * (i - 1) / 2 + (j - i);
+      P.S_out[q] = mulmod(reduce(atomicAdd(&P.gram_acc[qb], 0ull), M), P.gram_mul, M);
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < NP; q += kThreads) atomicExch(&P.gram_acc[q], 0ull);
   }
-  __syncthreads();
-  for (int q = threadIdx.x; q < NP; q += kThreads) atomicExch(&P.gram_acc[q], 0ull);
   if (threadIdx.x == 0) atomicExch(P.counter, 0u);
 }
 
@@ -648,6 +668,66 @@ static int occupancy_B(rr_krylov* kr, int* pass_blocks, int* chunk_blocks) {
     RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(chunk_blocks, chunk_kernel<B, 2>, kThreads, 0));
   }
   return RR_OK;
+}
+
+template <int B>
+static int launch_pass_raw_B(cudaStream_t s, int fold4, int grid, const PassParams& P, int mode) {
+  const size_t sm = pass_smem_bytes<B>();
+  const dim3 g(grid), block(kThreads);
+  if (fold4) {
+    if (mode == kModeInit) pass_kernel<B, kModeInit, 4><<<g, block, sm, s>>>(P);
+    else if (mode == kModeOdd) pass_kernel<B, kModeOdd, 4><<<g, block, sm, s>>>(P);
+    else pass_kernel<B, kModeEven, 4><<<g, block, sm, s>>>(P);
+  } else {
+    if (mode == kModeInit) pass_kernel<B, kModeInit, 2><<<g, block, sm, s>>>(P);
+    else if (mode == kModeOdd) pass_kernel<B, kModeOdd, 2><<<g, block, sm, s>>>(P);
+    else pass_kernel<B, kModeEven, 2><<<g, block, sm, s>>>(P);
+  }
+  RR_CUDA(cudaGetLastError());
+  return RR_OK;
+}
+
+int launch_pass_raw(cudaStream_t s, int B, int fold4, int grid, const PassParams& P, int mode) {
+  switch (B) {
+    case 4: return launch_pass_raw_B<4>(s, fold4, grid, P, mode);
+    case 8: return launch_pass_raw_B<8>(s, fold4, grid, P, mode);
+    case 16: return launch_pass_raw_B<16>(s, fold4, grid, P, mode);
+    case 32: return launch_pass_raw_B<32>(s, fold4, grid, P, mode);
+  }
+  return fail(RR_EINVAL, "unsupported padded block width %d", B);
+}
+
+template <int B>
+static int pass_blocks_B(int fold4, int* blocks) {
+  const size_t sm = pass_smem_bytes<B>();
+  if (fold4) {
+    RR_TRY((set_pass_smem<B, 4>()));
+    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, pass_kernel<B, kModeEven, 4>, kThreads, sm));
+  } else {
+    RR_TRY((set_pass_smem<B, 2>()));
+    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, pass_kernel<B, kModeEven, 2>, kThreads, sm));
+  }
+  return RR_OK;
+}
+
+int pass_blocks_per_sm(int B, int fold4, int* blocks) {
+  switch (B) {
+    case 4: return pass_blocks_B<4>(fold4, blocks);
+    case 8: return pass_blocks_B<8>(fold4, blocks);
+    case 16: return pass_blocks_B<16>(fold4, blocks);
+    case 32: return pass_blocks_B<32>(fold4, blocks);
+  }
+  return fail(RR_EINVAL, "unsupported padded block width %d", B);
+}
+
+int rows_per_batch(int B) {
+  switch (B) {
+    case 4: return Shape<4>::RPW;
+    case 8: return Shape<8>::RPW;
+    case 16: return Shape<16>::RPW;
+    case 32: return Shape<32>::RPW;
+  }
+  return 0;
 }
 
 int krylov_occupancy(rr_krylov* kr) {

@@ -1,0 +1,57 @@
+// krylov_params.h -- launch parameters of the Krylov pass kernels (krylov.cu),
+// shared with the batched engine (batch.cu).
+#pragma once
+#include "rr_internal.h"
+
+namespace rr {
+
+enum PassMode { kModeInit = 0, kModeOdd = 1, kModeEven = 2 };
+
+struct PassParams {
+  const uint32_t* rowptr;
+  const uint2* cv;          // packed (column, value)
+  int64_t rows;
+  int64_t heavy_rows;
+  const uint4* X;           // gathered block [cols][B/4]   (kModeInit: w [rows][B/4])
+  uint4* Y;                 // output block   [rows][B/4]
+  const uint32_t* scale;    // odd: d_r R^2; even: d_c R^2; init: d_c R   (all mod p)
+  const uint32_t* scale2;   // even: d_c R
+  unsigned long long* heavy_acc;  // [heavy_rows][B]
+  unsigned long long* gram_acc;   // [B(B+1)/2]
+  unsigned int* counter;
+  uint32_t* S_out;          // finished term, real pairs; nullptr = do not emit
+  uint32_t gram_mul;        // factor applied to the finished term
+  uint32_t w4, w5, w6;      // 2^32, 2^40, 2^48 mod p (limb weights of the tensor-core Gram)
+  int b_real;
+  ModP M;
+  // Batched mode (many matrices stacked block-diagonally, each padded to a
+  // multiple of 32 rows): batch_seg[batch] is the matrix of a row batch.  Warps
+  // then take contiguous runs of batches from batch_begin on, and Gram terms
+  // go to gram_acc[seg][NP] and to S_all + seg_S_off[seg] + term * np.
+  const int32_t* batch_seg; // nullptr: one matrix
+  int64_t batch_begin;
+  int32_t seg_begin, seg_end;
+  uint32_t* S_all;
+  const int64_t* seg_S_off;
+  int64_t term;
+};
+
+struct ChunkParams {
+  const uint2* cv;
+  const uint32_t* chunk_row;
+  const uint32_t* chunk_begin;
+  const uint32_t* chunk_end;
+  int64_t nchunks;
+  const uint4* X;
+  unsigned long long* heavy_acc;
+  ModP M;
+};
+
+// Launch one pass kernel for padded width B on stream s (grid = CTAs).
+int launch_pass_raw(cudaStream_t s, int B, int fold4, int grid, const PassParams& P, int mode);
+// CTAs per SM of the pass kernel for padded width B (also sets its shared-memory limit).
+int pass_blocks_per_sm(int B, int fold4, int* blocks);
+// Rows per warp batch for padded width B.
+int rows_per_batch(int B);
+
+}  // namespace rr

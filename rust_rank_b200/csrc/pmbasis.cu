@@ -694,17 +694,17 @@ int pm_basis_device(rr_ctx* ctx, const uint32_t* seq, int64_t seq_stride, int b,
       x = x * w % p;
       y = y * wi % p;
     }
-    RR_TRY(P.tw.alloc(nmax / 2));
-    RR_TRY(P.tws.alloc(nmax / 2));
-    RR_TRY(P.twi.alloc(nmax / 2));
-    RR_TRY(P.twis.alloc(nmax / 2));
+    RR_TRY(P.tw.alloc_async(nmax / 2, P.s));
+    RR_TRY(P.tws.alloc_async(nmax / 2, P.s));
+    RR_TRY(P.twi.alloc_async(nmax / 2, P.s));
+    RR_TRY(P.twis.alloc_async(nmax / 2, P.s));
     RR_CUDA(cudaMemcpyAsync(P.tw.ptr, t.data(), t.size() * 4, cudaMemcpyHostToDevice, P.s));
     RR_CUDA(cudaMemcpyAsync(P.tws.ptr, ts.data(), ts.size() * 4, cudaMemcpyHostToDevice, P.s));
     RR_CUDA(cudaMemcpyAsync(P.twi.ptr, ti.data(), ti.size() * 4, cudaMemcpyHostToDevice, P.s));
     RR_CUDA(cudaMemcpyAsync(P.twis.ptr, tis.data(), tis.size() * 4, cudaMemcpyHostToDevice, P.s));
-    RR_TRY(P.FA.alloc((size_t)m * m * nmax));
-    RR_TRY(P.FB.alloc((size_t)m * m * nmax));
-    RR_TRY(P.FC.alloc((size_t)m * m * nmax));
+    RR_TRY(P.FA.alloc_async((size_t)m * m * nmax, P.s));
+    RR_TRY(P.FB.alloc_async((size_t)m * m * nmax, P.s));
+    RR_TRY(P.FC.alloc_async((size_t)m * m * nmax, P.s));
     RR_CUDA(cudaStreamSynchronize(P.s));
   }
   // per-depth buffers
@@ -714,12 +714,12 @@ int pm_basis_device(rr_ctx* ctx, const uint32_t* seq, int64_t seq_stride, int b,
       const int64_t hl = dd / 2 + 1;
       for (int q = 0; q < 3; ++q) {
         P.bufs.emplace_back(new DevBuf<uint32_t>());
-        RR_TRY(P.bufs.back()->alloc((size_t)m * (q == 1 ? n : m) * hl));
+        RR_TRY(P.bufs.back()->alloc_async((size_t)m * (q == 1 ? n : m) * hl, P.s));
       }
     }
   }
-  RR_TRY(P.delta.alloc(m));
-  RR_TRY(P.status.alloc(1));
+  RR_TRY(P.delta.alloc_async(m, P.s));
+  RR_TRY(P.status.alloc_async(1, P.s));
   RR_CUDA(cudaMemsetAsync(P.delta.ptr, 0, m * sizeof(int64_t), P.s));
   RR_CUDA(cudaMemsetAsync(P.status.ptr, 0, sizeof(int), P.s));
   RR_TRY(set_base_smem_limit(P.base_smem));
@@ -727,13 +727,13 @@ int pm_basis_device(rr_ctx* ctx, const uint32_t* seq, int64_t seq_stride, int b,
   DevBuf<uint32_t> dseq, G;
   const int np = b * (b + 1) / 2;
   const int64_t glen = d + 1;
-  RR_TRY(dseq.alloc((size_t)np * glen));
+  RR_TRY(dseq.alloc_async((size_t)np * glen, P.s));
   RR_CUDA(cudaMemcpy2DAsync(dseq.ptr, glen * 4, seq, seq_stride * 4, glen * 4, np, cudaMemcpyHostToDevice, P.s));
-  RR_TRY(G.alloc((size_t)m * n * glen));
+  RR_TRY(G.alloc_async((size_t)m * n * glen, P.s));
   build_G_kernel<<<grid_for((int64_t)m * n * glen), 256, 0, P.s>>>(dseq.ptr, glen, b, glen, G.ptr, p);
   RR_CUDA(cudaGetLastError());
   DevBuf<uint32_t> Mo;
-  RR_TRY(Mo.alloc((size_t)m * m * (d + 1)));
+  RR_TRY(Mo.alloc_async((size_t)m * m * (d + 1), P.s));
   RR_TRY(pm_rec(P, G.ptr, (int64_t)n * glen, glen, d, 0, Mo.ptr, (int64_t)m * (d + 1), d + 1));
   int status = 0;
   RR_CUDA(cudaMemcpyAsync(Mh, Mo.ptr, Mo.bytes(), cudaMemcpyDeviceToHost, P.s));

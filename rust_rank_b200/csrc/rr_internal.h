@@ -40,14 +40,36 @@ template <class T>
 struct DevBuf {
   T* ptr = nullptr;
   size_t n = 0;
+  cudaStream_t stream = nullptr;  // set for stream-ordered buffers
+  bool ordered = false;
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
   ~DevBuf() { release(); }
   void release() {
-    if (ptr) cudaFree(ptr);
+    if (ptr) {
+      if (ordered) cudaFreeAsync(ptr, stream);
+      else cudaFree(ptr);
+    }
     ptr = nullptr;
     n = 0;
+    ordered = false;
+  }
+  // Stream-ordered allocation: no device-wide synchronisation on free, so
+  // work on other streams keeps running.
+  int alloc_async(size_t count, cudaStream_t s) {
+    release();
+    if (count == 0) return RR_OK;
+    cudaError_t e = cudaMallocAsync((void**)&ptr, count * sizeof(T), s);
+    if (e != cudaSuccess) {
+      ptr = nullptr;
+      cudaGetLastError();
+      return fail(RR_ENOMEM, "cudaMallocAsync of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
+    }
+    n = count;
+    stream = s;
+    ordered = true;
+    return RR_OK;
   }
   int alloc(size_t count) {
     release();

@@ -162,6 +162,59 @@ def incidence(m: int, n: int, kmin: int = 3, kmax: int = 10, deficit: int = 0, p
     return rowptr, col, val, m, n
 
 
+def incidence_fast(m: int, n: int, kmin: int = 3, kmax: int = 10, col_deficit: int = 0, p: int = P_DEFAULT,
+                   seed: int = 46):
+    """Vectorised signed-incidence style matrix for large batches.
+
+    Row r draws kmin..kmax columns uniformly (a repeated draw is dropped, so a
+    row may come out one entry short) with values +-1.  Then ``col_deficit``
+    columns are overwritten by copies of other columns, so the rank is at most
+    n - col_deficit (the matrices are tall, so dependent rows would not lower
+    the rank).
+    """
+    rng = np.random.default_rng(seed)
+    lens = rng.integers(kmin, kmax + 1, size=m)
+    cand = np.sort(rng.integers(0, n, size=(m, kmax), dtype=np.int64), axis=1)
+    keep = np.arange(kmax)[None, :] < lens[:, None]
+    keep[:, 1:] &= cand[:, 1:] != cand[:, :-1]
+    rows = np.broadcast_to(np.arange(m, dtype=np.int64)[:, None], cand.shape)[keep]
+    cols = cand[keep]
+    vals = rng.integers(0, 2, size=cols.size, dtype=np.int64) * 2 - 1
+    if col_deficit > 0:
+        pick = rng.permutation(n)[: 2 * col_deficit]
+        src, dst = pick[:col_deficit], pick[col_deficit:]
+        drop = np.isin(cols, dst)
+        rows, cols, vals = rows[~drop], cols[~drop], vals[~drop]
+        where = np.full(n, -1, np.int64)
+        where[src] = dst
+        sel = where[cols] >= 0
+        rows = np.concatenate([rows, rows[sel]])
+        vals = np.concatenate([vals, vals[sel]])
+        cols = np.concatenate([cols, where[cols[sel]]])
+    order = np.lexsort((cols, rows))
+    rows, cols, vals = rows[order], cols[order], vals[order]
+    rowptr = np.zeros(m + 1, np.int64)
+    rowptr[1:] = np.cumsum(np.bincount(rows, minlength=m))
+    return rowptr, cols.astype(np.int32), (vals % p).astype(np.uint32), m, n
+
+
+def graph_complex_batch(nmat: int = 256, rmin: int = 1000, rmax: int = 200_000, kmin: int = 3, kmax: int = 10,
+                        deficit_every: int = 8, p: int = P_DEFAULT, seed: int = 47):
+    """Config 3: ``nmat`` incidence-style matrices, rows log-uniform in
+    [rmin, rmax], columns = rows * U(0.6, 1.0); every ``deficit_every``-th
+    matrix gets a planted column deficit of about 1% of its columns."""
+    rng = np.random.default_rng(seed)
+    rows = np.exp(rng.uniform(np.log(rmin), np.log(rmax), size=nmat)).astype(np.int64)
+    frac = rng.uniform(0.6, 1.0, size=nmat)
+    mats = []
+    for i in range(nmat):
+        m = int(rows[i])
+        n = max(1, int(m * frac[i]))
+        dfc = (n // 100 + 1) if deficit_every and i % deficit_every == 0 else 0
+        mats.append(incidence_fast(m, n, kmin, kmax, dfc, p, seed * 1000 + i))
+    return mats
+
+
 def random_vectors(b: int, n: int, p: int, seed: int, nonzero: bool = False) -> np.ndarray:
     """b x n uniform in [0, p) (or [1, p) with nonzero), like src/matrices.rs:484-497."""
     rng = np.random.default_rng(seed)
