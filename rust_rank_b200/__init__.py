@@ -15,13 +15,35 @@ beyond argument marshalling.
 """
 from __future__ import annotations
 
+import atexit
+import ctypes as C
 import time
+import weakref
 from dataclasses import dataclass
 
 import numpy as np
 
 from ._lib import RRError, check, lib, ptr  # noqa: F401
-import ctypes as C
+
+# Live handles by teardown order (states and batches, then matrices, then
+# contexts): closed at interpreter exit before module teardown, so a handle is
+# never destroyed after the context it lives on.
+_LIVE = (weakref.WeakSet(), weakref.WeakSet(), weakref.WeakSet())
+
+
+def _track(obj, level: int):
+    _LIVE[level].add(obj)
+
+
+@atexit.register
+def _close_all():
+    for group in _LIVE:
+        for obj in list(group):
+            try:
+                obj.close()
+            except Exception:
+                pass
+
 
 __all__ = ["Context", "CsrMatrix", "DeviceMatrix", "KrylovStream", "main_loop_s_mt2", "PM_Basis",
            "analyze_pm_basis", "block_wiedemann_rank", "save_wdm_file_sym", "load_wdm_file_sym",
@@ -37,6 +59,7 @@ class Context:
         h = C.c_void_p()
         check(lib().rr_ctx_create(device, C.byref(h)))
         self.handle = h
+        _track(self, 2)
         self.device = device
 
     @property
@@ -117,6 +140,7 @@ class DeviceMatrix:
         check(lib().rr_matrix_create(ctx.handle, a.n_rows, a.n_cols, ptr(a.row_ptr), ptr(a.col_indices),
                                      ptr(a.values), self.p, C.byref(h)))
         self.handle = h
+        _track(self, 1)
 
     def max_nnzs(self):
         r, c = C.c_int64(), C.c_int64()
@@ -154,6 +178,7 @@ class KrylovStream:
         check(lib().rr_krylov_create(a.handle, self.b, ptr(self.row_precond), ptr(self.col_precond), ptr(curv),
                                      int(seq_len), C.byref(h)))
         self.handle = h
+        _track(self, 0)
 
     def __len__(self) -> int:
         v = C.c_int64()
@@ -329,6 +354,7 @@ class Batch:
         check(lib().rr_batch_create(self.ctx.handle, self.n, ptr(m), ptr(n), rp, cl, vl, int(theprime), self.b, rpc,
                                     cpc, vv, C.byref(h)))
         self.handle = h
+        _track(self, 0)
 
     def krylov(self):
         check(lib().rr_batch_krylov(self.handle))

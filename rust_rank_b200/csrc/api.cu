@@ -6,7 +6,7 @@
 #include <cstring>
 #include <memory>
 
-#include "rr_internal.h"
+#include "krylov_params.h"
 
 namespace rr {
 
@@ -268,7 +268,7 @@ int rr_krylov_create(rr_matrix* mat, int32_t b, const uint32_t* row_precond, con
   const int64_t heavy = std::max<int64_t>(std::max(mat->A.heavy_rows, mat->At.heavy_rows), 1);
   RR_TRY(kr->heavy_acc.alloc((size_t)heavy * B));
   RR_CUDA(cudaMemsetAsync(kr->heavy_acc.ptr, 0, kr->heavy_acc.bytes(), s));
-  RR_TRY(kr->gram_acc.alloc(B * (B + 1) / 2));
+  RR_TRY(kr->gram_acc.alloc((size_t)kGramReplicas * (B * (B + 1) / 2)));
   RR_CUDA(cudaMemsetAsync(kr->gram_acc.ptr, 0, kr->gram_acc.bytes(), s));
   RR_TRY(kr->counter.alloc(4));
   RR_CUDA(cudaMemsetAsync(kr->counter.ptr, 0, kr->counter.bytes(), s));

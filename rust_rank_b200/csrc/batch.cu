@@ -41,6 +41,10 @@ struct rr_batch_s {
   std::vector<int64_t> s_off;    // sequence offset (words) per stack position
   rr::DevCsr A, At;
   rr::DevBuf<int32_t> seg_rows, seg_cols;  // matrix of each row batch of A / A^T
+  // equal-work warp runs per phase (a phase = a set of running matrices):
+  // runs_*[phase][warp], kPassWarps * grid + 1 entries each
+  rr::DevBuf<int32_t> runs_rows, runs_cols;
+  std::vector<int> phase_of;  // first running stack position -> phase
   rr::DevBuf<uint32_t> X[2], U, dr_m, dc_m, dc_r, W0;
   rr::DevBuf<unsigned long long> gram_acc;
   rr::DevBuf<unsigned int> counter;
@@ -73,6 +77,8 @@ PassParams batch_params(rr_batch* bt) {
   PassParams P;
   std::memset(&P, 0, sizeof(P));
   P.gram_acc = bt->gram_acc.ptr;
+  P.gram_stride = (int64_t)bt->nmat * (bt->B * (bt->B + 1) / 2);
+  P.replicas = 1;
   P.counter = bt->counter.ptr;
   P.gram_mul = 1;
   P.w4 = bt->M.c32;
@@ -86,6 +92,31 @@ PassParams batch_params(rr_batch* bt) {
   return P;
 }
 
+
+// Work of a row: its nonzeros plus a fixed cost for the row's epilogue and
+// Gram contribution, in units of one gathered nonzero.
+constexpr int64_t kRowCost = 3;
+
+// Boundaries that split batches [qb, nb) into `nw` contiguous runs of about
+// equal work (prefix = work prefix over batches).
+void equal_runs(const std::vector<int64_t>& prefix, int64_t qb, int64_t nb, int nw, int32_t* out) {
+  const int64_t base = prefix[qb], total = prefix[nb] - base;
+  int64_t q = qb;
+  for (int w = 0; w <= nw; ++w) {
+    const int64_t target = base + (int64_t)((unsigned __int128)total * (uint64_t)w / (uint64_t)nw);
+    while (q < nb && prefix[q] < target) ++q;
+    out[w] = (int32_t)q;
+  }
+  out[nw] = (int32_t)nb;
+}
+
+std::vector<int64_t> batch_work(const std::vector<uint32_t>& ptr, int rpb) {
+  const int64_t rows = (int64_t)ptr.size() - 1, nb = rows / rpb;
+  std::vector<int64_t> pre(nb + 1, 0);
+  for (int64_t q = 0; q < nb; ++q)
+    pre[q + 1] = pre[q] + (int64_t)(ptr[(q + 1) * rpb] - ptr[q * rpb]) + kRowCost * rpb;
+  return pre;
+}
 
 // Completion of the sequences as the Krylov loop publishes them.
 struct Progress {
@@ -119,11 +150,14 @@ int krylov_run(rr_batch* bt, cudaEvent_t* ev, Progress* prog) {
   int first = 0;
   for (int64_t t = 0; t < max_apps; ++t) {
     while (first < nmat && bt->apps[first] <= t) ++first;
+    const size_t run_off = (size_t)bt->phase_of[first] * (bt->grid * kPassWarps + 1);
     uint32_t* x = bt->X[bt->cur].ptr;
     uint32_t* xn = bt->X[bt->cur ^ 1].ptr;
     PassParams P = batch_params(bt);
     P.seg_begin = first;
     P.seg_end = nmat;
+    // few running matrices: spread their accumulators over replicas
+    P.replicas = std::max(1, std::min(kGramReplicas, 64 / (nmat - first)));
     // rows of A: z = A x, U = D_r z, odd term
     P.rowptr = bt->A.rowptr.ptr;
     P.cv = bt->A.cv.ptr;
@@ -133,6 +167,7 @@ int krylov_run(rr_batch* bt, cudaEvent_t* ev, Progress* prog) {
     P.scale = bt->dr_m.ptr;
     P.gram_mul = bt->M.r1;
     P.batch_seg = bt->seg_rows.ptr;
+    P.runs = bt->runs_rows.ptr + run_off;
     P.batch_begin = bt->row_off[first] / rpb;
     P.term = 2 * t + 1;
     RR_TRY(launch_pass_raw(st, bt->B, bt->fold4, bt->grid, P, kModeOdd));
@@ -146,6 +181,7 @@ int krylov_run(rr_batch* bt, cudaEvent_t* ev, Progress* prog) {
     P.scale2 = bt->dc_r.ptr;
     P.gram_mul = 1;
     P.batch_seg = bt->seg_cols.ptr;
+    P.runs = bt->runs_cols.ptr + run_off;
     P.batch_begin = bt->col_off[first] / rpb;
     P.term = 2 * t + 2;
     RR_TRY(launch_pass_raw(st, bt->B, bt->fold4, bt->grid, P, kModeEven));
@@ -317,7 +353,7 @@ int rr_batch_create(rr_ctx* ctx, int32_t nmat, const int64_t* m, const int64_t* 
   RR_TRY(bt->X[1].alloc((size_t)Ntot * bt->B));
   RR_TRY(bt->U.alloc((size_t)Mtot * bt->B));
   const int NP = bt->B * (bt->B + 1) / 2;
-  RR_TRY(bt->gram_acc.alloc((size_t)nmat * NP));
+  RR_TRY(bt->gram_acc.alloc((size_t)kGramReplicas * nmat * NP));
   RR_CUDA(cudaMemsetAsync(bt->gram_acc.ptr, 0, bt->gram_acc.bytes(), st));
   RR_TRY(bt->counter.alloc(4));
   RR_CUDA(cudaMemsetAsync(bt->counter.ptr, 0, bt->counter.bytes(), st));
@@ -325,6 +361,25 @@ int rr_batch_create(rr_ctx* ctx, int32_t nmat, const int64_t* m, const int64_t* 
   int blocks = 1;
   RR_TRY(pass_blocks_per_sm(bt->B, bt->fold4, &blocks));
   bt->grid = std::max(1, blocks) * ctx->num_sms;
+  {  // phases: one per distinct set of running matrices
+    const int nw = bt->grid * kPassWarps;
+    std::vector<int> firsts;
+    bt->phase_of.assign(nmat, -1);
+    for (int s = 0; s < nmat; ++s)
+      if (s == 0 || bt->apps[s] != bt->apps[s - 1]) {
+        bt->phase_of[s] = (int)firsts.size();
+        firsts.push_back(s);
+      }
+    const std::vector<int64_t> wa = batch_work(aptr, rpb), wt = batch_work(tptr, rpb);
+    std::vector<int32_t> ra(firsts.size() * (nw + 1)), rt(firsts.size() * (nw + 1));
+    for (size_t ph = 0; ph < firsts.size(); ++ph) {
+      const int f = firsts[ph];
+      equal_runs(wa, bt->row_off[f] / rpb, Mtot / rpb, nw, ra.data() + ph * (nw + 1));
+      equal_runs(wt, bt->col_off[f] / rpb, Ntot / rpb, nw, rt.data() + ph * (nw + 1));
+    }
+    RR_TRY(up(bt->runs_rows, ra));
+    RR_TRY(up(bt->runs_cols, rt));
+  }
   int prio_lo = 0, prio_hi = 0;
   RR_CUDA(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
   RR_CUDA(cudaStreamCreateWithPriority(&bt->stream, cudaStreamNonBlocking, prio_hi));

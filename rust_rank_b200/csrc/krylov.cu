@@ -43,6 +43,7 @@ namespace rr {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
+static_assert(kWarps == kPassWarps, "host-side run tables assume this many warps per CTA");
 
 template <int B>
 struct Shape {
@@ -394,6 +395,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass_kernel(PassParams P) {
   for (int q = threadIdx.x; q < NP; q += kThreads) red[q] = 0;
   Gram gram;
   if (P.S_out != nullptr) gram.init(gram_smem + (size_t)warp * Gram::kWords, lane);
+  __syncthreads();  // red[] zeroed before a warp may emit into it
 
   const int64_t nbatch = (P.rows + RPW - 1) / RPW;
   const int64_t gw = (int64_t)blockIdx.x * kWarps + warp;
@@ -403,13 +405,28 @@ __global__ void __launch_bounds__(kThreads, 4) pass_kernel(PassParams P) {
   // runs, so that a warp changes matrix (and flushes its Gram terms) rarely
   int64_t b_first = gw, b_stop = nbatch, b_step = nw;
   if (segmented) {
-    const int64_t total = nbatch - P.batch_begin;
-    const int64_t q = (total + nw - 1) / nw;
-    b_first = P.batch_begin + gw * q;
-    b_stop = b_first + q < nbatch ? b_first + q : nbatch;
+    if (P.runs != nullptr) {  // runs of equal work (nonzeros + rows), built on the host
+      b_first = P.runs[gw];
+      b_stop = P.runs[gw + 1];
+    } else {
+      const int64_t total = nbatch - P.batch_begin;
+      const int64_t q = (total + nw - 1) / nw;
+      b_first = P.batch_begin + gw * q;
+      b_stop = b_first + q < nbatch ? b_first + q : nbatch;
+    }
     b_step = 1;
   }
   int cur_seg = -1;
+  // batched: the CTA's first matrix is reduced in shared memory (red), any
+  // other matrix a warp meets goes straight to the accumulators
+  int seg0 = -1;
+  unsigned long long* const acc = P.gram_acc + (size_t)(blockIdx.x % P.replicas) * P.gram_stride;
+  if (segmented) {
+    const int64_t lo = P.runs != nullptr ? (int64_t)P.runs[(int64_t)blockIdx.x * kWarps]
+                                         : P.batch_begin + (int64_t)blockIdx.x * kWarps *
+                                                               ((nbatch - P.batch_begin + nw - 1) / nw);
+    if (lo < nbatch) seg0 = P.batch_seg[lo];
+  }
 
   for (int64_t batch = b_first; batch < b_stop; batch += b_step) {
     if (segmented && P.S_out != nullptr) {
@@ -417,7 +434,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass_kernel(PassParams P) {
       if (sg != cur_seg) {
         if (cur_seg >= 0) {
           gram.finish(slot, sub, lane, M, W);
-          gram.emit(P.gram_acc + (size_t)cur_seg * NP, lane, M);
+          gram.emit(cur_seg == seg0 ? red : acc + (size_t)cur_seg * NP, lane, M);
           gram.reset();
         }
         cur_seg = sg;
@@ -490,13 +507,16 @@ __global__ void __launch_bounds__(kThreads, 4) pass_kernel(PassParams P) {
 
   if (P.S_out == nullptr) return;
   gram.finish(slot, sub, lane, M, W);
+  __syncthreads();  // red[] is zeroed before any warp emits into it
   if (segmented) {
-    if (cur_seg >= 0) gram.emit(P.gram_acc + (size_t)cur_seg * NP, lane, M);
-  } else {
+    if (cur_seg >= 0) gram.emit(cur_seg == seg0 ? red : acc + (size_t)cur_seg * NP, lane, M);
     __syncthreads();
+    if (seg0 >= 0)
+      for (int q = threadIdx.x; q < NP; q += kThreads) atomicAdd(&acc[(size_t)seg0 * NP + q], red[q]);
+  } else {
     gram.emit(red, lane, M);
     __syncthreads();
-    for (int q = threadIdx.x; q < NP; q += kThreads) atomicAdd(&P.gram_acc[q], red[q]);
+    for (int q = threadIdx.x; q < NP; q += kThreads) atomicAdd(&acc[q], red[q]);
   }
   __threadfence();
   __syncthreads();
@@ -508,23 +528,48 @@ __global__ void __launch_bounds__(kThreads, 4) pass_kernel(PassParams P) {
   const int b = P.b_real;
   const int npr = b * (b + 1) / 2;
   if (segmented) {
+    // every other CTA's atomics are visible (fence + counter), so plain L2
+    // loads suffice; four in flight per thread
     const int nseg = P.seg_end - P.seg_begin;
-    for (int64_t e = threadIdx.x; e < (int64_t)nseg * npr; e += kThreads) {
-      const int s = P.seg_begin + (int)(e / npr), q = (int)(e % npr);
-      int i, j;
-      pair_of(q, b, i, j);
-      unsigned long long* g = P.gram_acc + (size_t)s * NP + pair_index(i, j, B);
-      P.S_all[P.seg_S_off[s] + P.term * npr + q] = mulmod(reduce(atomicExch(g, 0ull), M), P.gram_mul, M);
+    const int64_t total = (int64_t)nseg * npr;
+    for (int64_t e0 = threadIdx.x; e0 < total; e0 += 4 * kThreads) {
+      unsigned long long v[4];
+      unsigned long long* g[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int64_t e = e0 + (int64_t)u * kThreads;
+        g[u] = nullptr;
+        if (e < total) {
+          const int s = P.seg_begin + (int)(e / npr), q = (int)(e % npr);
+          int i, j;
+          pair_of(q, b, i, j);
+          g[u] = P.gram_acc + (size_t)s * NP + pair_index(i, j, B);
+          v[u] = 0;
+          for (int r = 0; r < P.replicas; ++r) v[u] += __ldcg(g[u] + (size_t)r * P.gram_stride);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int64_t e = e0 + (int64_t)u * kThreads;
+        if (g[u] != nullptr) {
+          const int s = P.seg_begin + (int)(e / npr), q = (int)(e % npr);
+          P.S_all[P.seg_S_off[s] + P.term * npr + q] = mulmod(reduce(v[u], M), P.gram_mul, M);
+          for (int r = 0; r < P.replicas; ++r) __stcg(g[u] + (size_t)r * P.gram_stride, 0ull);
+        }
+      }
     }
   } else {
     for (int q = threadIdx.x; q < npr; q += kThreads) {
       int i, j;
       pair_of(q, b, i, j);
-      const int qb = i * B - i * (i - 1) / 2 + (j - i);
-      P.S_out[q] = mulmod(reduce(atomicAdd(&P.gram_acc[qb], 0ull), M), P.gram_mul, M);
+      const int qb = pair_index(i, j, B);
+      unsigned long long v = 0;
+      for (int r = 0; r < P.replicas; ++r) v += __ldcg(P.gram_acc + (size_t)r * P.gram_stride + qb);
+      P.S_out[q] = mulmod(reduce(v, M), P.gram_mul, M);
     }
     __syncthreads();
-    for (int q = threadIdx.x; q < NP; q += kThreads) atomicExch(&P.gram_acc[q], 0ull);
+    for (int q = threadIdx.x; q < NP * P.replicas; q += kThreads)
+      __stcg(P.gram_acc + (size_t)(q / NP) * P.gram_stride + q % NP, 0ull);
   }
   if (threadIdx.x == 0) atomicExch(P.counter, 0u);
 }
@@ -750,6 +795,8 @@ static PassParams base_params(rr_krylov* kr) {
   std::memset(&P, 0, sizeof(P));
   P.heavy_acc = kr->heavy_acc.ptr;
   P.gram_acc = kr->gram_acc.ptr;
+  P.gram_stride = kr->B * (kr->B + 1) / 2;
+  P.replicas = kGramReplicas;
   P.counter = kr->counter.ptr;
   P.gram_mul = 1;
   P.w4 = kr->M.c32;

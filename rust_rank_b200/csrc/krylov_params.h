@@ -17,7 +17,9 @@ struct PassParams {
   const uint32_t* scale;    // odd: d_r R^2; even: d_c R^2; init: d_c R   (all mod p)
   const uint32_t* scale2;   // even: d_c R
   unsigned long long* heavy_acc;  // [heavy_rows][B]
-  unsigned long long* gram_acc;   // [B(B+1)/2]
+  unsigned long long* gram_acc;   // [replicas][segments][B(B+1)/2]; CTA c adds into replica c % replicas
+  int64_t gram_stride;            // words per replica (segments * B(B+1)/2)
+  int replicas;                   // 1..kGramReplicas
   unsigned int* counter;
   uint32_t* S_out;          // finished term, real pairs; nullptr = do not emit
   uint32_t gram_mul;        // factor applied to the finished term
@@ -29,6 +31,7 @@ struct PassParams {
   // then take contiguous runs of batches from batch_begin on, and Gram terms
   // go to gram_acc[seg][NP] and to S_all + seg_S_off[seg] + term * np.
   const int32_t* batch_seg; // nullptr: one matrix
+  const int32_t* runs;      // batched: warp w takes batches [runs[w], runs[w+1]); nullptr = equal counts
   int64_t batch_begin;
   int32_t seg_begin, seg_end;
   uint32_t* S_all;
@@ -53,5 +56,10 @@ int launch_pass_raw(cudaStream_t s, int B, int fold4, int grid, const PassParams
 int pass_blocks_per_sm(int B, int fold4, int* blocks);
 // Rows per warp batch for padded width B.
 int rows_per_batch(int B);
+// Warps per CTA of the pass kernel.
+constexpr int kPassWarps = 8;
+// Copies of the Gram accumulators: CTAs spread their 64-bit atomics over
+// this many copies so that no L2 slice serialises all of them.
+constexpr int kGramReplicas = 8;
 
 }  // namespace rr
