@@ -491,6 +491,676 @@ size_t base_smem_bytes(int m, int n, int K, bool m_smem) {
   return bytes;
 }
 
+// ---------------------------------------------------------------- leaves + block basis (main path)
+// The main path splits a block of K leaves in two kernels:
+//
+//   pm_leaves_kernel (one CTA) runs the K order-1 leaves in sequence and, for
+//   each, records the stored transform T_k (transposed, Tt[k][s][i]) and its
+//   pivot rows; it updates only the residual series, which is what the next
+//   leaf depends on.
+//   pm_block_basis_kernel (one CTA per basis column) multiplies the recorded
+//   factors m_{K-1} ... m_0 (m_k = D1 T_k + x Dx T_k) in parallel and writes the
+//   block's basis, normalised by the row scales.
+//
+// Elimination.  For m <= 32 rows and n + m <= 48 columns (b <= 16) one warp
+// eliminates with one row per lane, held in registers: the pivot row is
+// broadcast by shuffles, the pivot column is the unpivoted column of least
+// list position (one redux.sync), and no CTA barrier is needed.  Larger
+// blocks keep the matrix in shared memory and give each warp the rows
+// i == warp (mod 16), with one CTA barrier per pivot step.  Either way the
+// loop stops once all n columns have pivots: no later row can get one.
+//
+// Residual update.  The rows are regrouped so that pivot rows ("x" rows,
+// shifted by one coefficient) come first, each group padded to a multiple of
+// four; a thread then computes a 4 x 4 tile (16 independent 64-bit
+// accumulators) whose rows all read the same source coefficient.
+constexpr int kLeafThreads = 512;
+constexpr int kLeafWarps = kLeafThreads / 32;
+
+
+struct LeafParams {
+  const uint32_t* G;  // G[i][c][t] (row stride g_rs, column stride g_cs), t < K
+  int64_t g_rs, g_cs;
+  int m, n, K;
+  int64_t cs;                // words per residual coefficient in shared memory (>= m * n, padded)
+  int64_t* delta;            // [m], in/out
+  uint32_t* Tt;              // [K][m][m]: Tt[k][s][i] = stored T_k[i][s]
+  unsigned long long* mask;  // [K]: bit i set when row i of leaf k is a pivot row (an "x" row)
+  uint32_t* sigma_inv;       // [m]: inverse row scales of the block's stored basis
+  ModP M;
+  int* status;
+};
+
+// Row stride (words) of the slot-ordered transform in shared memory: room for
+// m rows plus the padding of two groups, a multiple of four.
+__host__ __device__ constexpr int leaf_tstride(int m) { return (m + 6 + 3) & ~3; }
+
+// Shared-memory bytes of pm_leaves_kernel.
+size_t leaves_smem_bytes(int m, int n, int K, int64_t cs) {
+  const size_t W = (size_t)n + m, TS = (size_t)leaf_tstride(m);
+  size_t words = (size_t)2 * K * cs + (((size_t)m * W + 3) & ~(size_t)3) + (size_t)m * TS + 2 * (size_t)m;
+  size_t bytes = (words * 4 + 15) & ~(size_t)15;
+  bytes += 2 * (size_t)m * 8 + (3 * (size_t)m + (size_t)n + TS) * 4 + 64;
+  return bytes;
+}
+
+// Shared-memory bytes of pm_block_basis_kernel.
+size_t block_basis_smem_bytes(int m, int K) {
+  const size_t S = (size_t)leaf_tstride(m), VS = ((size_t)(K + 1) * (m + 1) + 3) & ~(size_t)3;
+  return (2 * VS + (size_t)m * S) * 4 + (size_t)S * 4;
+}
+
+// Pivot search of row r by one warp (src/modular_linalg.rs:198-226): the first
+// non-zero column of row r in the order of the unpivoted list Lst.  A pivot
+// moves the list's front into the pivot's slot and pops the front.
+__device__ __forceinline__ void leaf_search(int r, const uint32_t* A, int W, int n, int* Lst, int* s_flag,
+                                            int* s_col, int* s_rank, int* rowmask, int lane) {
+  const int rank = r == 0 ? 0 : s_rank[(r - 1) & 1];
+  const int len = n - rank;
+  int c = -1;
+  bool nz = false;
+  if (lane < len) {
+    c = Lst[lane];
+    nz = A[r * W + c] != 0;
+  }
+  const unsigned bal = __ballot_sync(0xffffffffu, nz);
+  const int l0 = __shfl_sync(0xffffffffu, c, 0);
+  const int nxt = __shfl_down_sync(0xffffffffu, c, 1);
+  int col = 0;
+  if (bal) {
+    const int ts = __ffs(bal) - 1;
+    col = __shfl_sync(0xffffffffu, c, ts);
+    __syncwarp();
+    if (lane < len - 1) Lst[lane] = (lane == ts - 1) ? l0 : nxt;
+  }
+  if (lane == 0) {
+    s_flag[r & 1] = bal ? 1 : 0;
+    s_col[r & 1] = col;
+    s_rank[r & 1] = rank + (bal ? 1 : 0);
+    rowmask[r] = bal ? 1 : 0;
+  }
+}
+
+// Slot of row i (i < m) in the grouped order: pivot rows first (increasing
+// i), padded to a multiple of four, then the other rows.  mx is the pivot-row
+// mask; rows past m never get a slot.
+__device__ __forceinline__ int leaf_slot(unsigned long long mx, int i, int m) {
+  const unsigned long long below = (i == 0) ? 0ull : (~0ull >> (64 - i));
+  const int nx = __popcll(mx);
+  if ((mx >> i) & 1ull) return __popcll(mx & below);
+  const unsigned long long valid = (m == 64) ? ~0ull : ((1ull << m) - 1);
+  return ((nx + 3) & ~3) + __popcll(~mx & valid & below);
+}
+
+template <int CT, int FE>
+__global__ void __launch_bounds__(kLeafThreads) pm_leaves_kernel(LeafParams P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int m = P.m, n = P.n, K = P.K;
+  const int W = n + m;
+  const int TS = leaf_tstride(m);
+  const int CS = (int)P.cs;
+  const ModP M = P.M;
+  const uint32_t p = M.p;
+  uint32_t* Rc = reinterpret_cast<uint32_t*>(smem_raw);  // [K][CS]: residual coefficient t, row i, column c
+  uint32_t* Rn = Rc + (size_t)K * CS;
+  uint32_t* A = Rn + (size_t)K * CS;                      // m x W augmented matrix [pi r | pi] (multi-warp path)
+  uint32_t* Tq = A + ((m * W + 3) & ~3);                  // m x TS: Tq[s][slot] = T[row(slot)][s]
+  uint32_t* sigma = Tq + m * TS;                          // m
+  uint32_t* sig_tmp = sigma + m;                          // m
+  const size_t w32 = (size_t)2 * K * CS + (((size_t)m * W + 3) & ~(size_t)3) + (size_t)m * TS + 2 * (size_t)m;
+  int64_t* sdelta = reinterpret_cast<int64_t*>(smem_raw + ((w32 * 4 + 15) & ~(size_t)15));
+  int64_t* sdelta_tmp = sdelta + m;
+  int* perm = reinterpret_cast<int*>(sdelta_tmp + m);
+  int* rowmask = perm + m;
+  int* slotrow = rowmask + m;  // TS entries: row of a slot, -1 for padding
+  int* Lst = slotrow + TS;
+  __shared__ int s_flag[2], s_col[2], s_rank[2];
+  __shared__ unsigned long long s_mx;
+
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5;
+
+  for (int i = warp; i < m; i += kLeafWarps)
+    for (int c = lane; c < n; c += 32)
+      for (int t = 0; t < K; ++t) Rc[t * CS + i * n + c] = P.G[(int64_t)i * P.g_rs + (int64_t)c * P.g_cs + t];
+  for (int i = tid; i < m; i += nt) {
+    sdelta[i] = P.delta[i];
+    sigma[i] = 1;
+  }
+  __syncthreads();
+
+  for (int leaf = 0; leaf < K; ++leaf) {
+    uint32_t* Tg = P.Tt + (size_t)leaf * m * m;
+    // stable sort of delta, descending (src/sigma_basis.rs:357-359)
+    for (int i = tid; i < m; i += nt) {
+      const int64_t di = sdelta[i];
+      int pos = 0;
+      for (int j = 0; j < m; ++j) {
+        const int64_t dj = sdelta[j];
+        pos += (dj > di) || (dj == di && j < i);
+      }
+      perm[pos] = i;
+    }
+    for (int i = tid; i < n; i += nt) Lst[i] = i;
+    for (int i = tid; i < m; i += nt) rowmask[i] = 0;
+    __syncthreads();
+    // A = [pi r | pi]  (src/sigma_basis.rs:369-380)
+    for (int i = warp; i < m; i += kLeafWarps) {
+      const int pi = perm[i];
+      for (int c = lane; c < W; c += 32) A[i * W + c] = c < n ? Rc[pi * n + c] : ((c - n) == pi ? 1u : 0u);
+    }
+    __syncthreads();
+    if (warp == 0) leaf_search(0, A, W, n, Lst, s_flag, s_col, s_rank, rowmask, lane);
+    // LSP elimination, fraction-free: row_i <- (piv row_i - a_i,cs row_k) R^{-1}
+    for (int k = 0; k < m; ++k) {
+      __syncthreads();  // row k final, its pivot published
+      const int flag = s_flag[k & 1], cs = s_col[k & 1];
+      const int rank_k = s_rank[k & 1];
+      if (flag) {
+        const uint32_t* ak = A + k * W;
+        const uint32_t piv = ak[cs];
+        int i = warp;
+        while (i <= k) i += kLeafWarps;
+        for (; i < m; i += kLeafWarps) {
+          uint32_t* ai = A + i * W;
+          const uint32_t f = ai[cs];
+          __syncwarp();
+          const uint64_t nf = (uint64_t)(p - f);
+          for (int c = lane; c < W; c += 32) ai[c] = redc(mad_wide(piv, ai[c], nf * ak[c]), M);
+        }
+      }
+      if (rank_k == n) break;  // every column has its pivot: no later row pivots
+      if (k + 1 < m && warp == (k + 1) % kLeafWarps) {
+        __syncwarp();
+        leaf_search(k + 1, A, W, n, Lst, s_flag, s_col, s_rank, rowmask, lane);
+      }
+    }
+    __syncthreads();
+    if (warp == 0) {
+      unsigned long long mx = 0;
+      for (int i = lane; i < m; i += 32) mx |= (unsigned long long)(rowmask[i] != 0) << i;
+#pragma unroll
+      for (int off = 16; off; off >>= 1) mx |= __shfl_xor_sync(0xffffffffu, mx, off);
+      if (lane == 0) {
+        P.mask[leaf] = mx;
+        s_mx = mx;
+      }
+      for (int q = lane; q < TS; q += 32) slotrow[q] = -1;
+    }
+    __syncthreads();
+    const unsigned long long mx = s_mx;
+    for (int i = tid; i < m; i += nt) slotrow[leaf_slot(mx, i, m)] = i;
+    for (int e = tid; e < m * TS; e += nt) Tq[e] = 0;
+    __syncthreads();
+    for (int i = warp; i < m; i += kLeafWarps) {
+      const int slot = leaf_slot(mx, i, m);
+      for (int s = lane; s < m; s += 32) {
+        const uint32_t v = A[i * W + n + s];
+        Tq[s * TS + slot] = v;
+        Tg[s * m + i] = v;
+      }
+    }
+    for (int i = tid; i < m; i += nt) {
+      const uint32_t ci = A[i * W + n + perm[i]];
+      if (ci == 0) atomicExch(P.status, 2);
+      sig_tmp[i] = redc((uint64_t)ci * sigma[perm[i]], M);
+      sdelta_tmp[i] = sdelta[perm[i]] - rowmask[i];  // src/sigma_basis.rs:408-411
+    }
+    __syncthreads();
+    for (int i = tid; i < m; i += nt) {
+      sigma[i] = sig_tmp[i];
+      sdelta[i] = sdelta_tmp[i];
+    }
+    __syncthreads();
+    // residual: Rn[t][i] = T_i . Rc[t + 1 - mask_i], t < K - leaf - 1, in 4 x CT tiles
+    const int rem = K - leaf - 1;
+    if (rem > 0) {
+      const unsigned long long mx = s_mx;
+      const int nx = __popcll(mx);
+      const int gx = (nx + 3) & ~3;
+      const int QG = (gx + ((m - nx + 3) & ~3)) / 4, CG = n / CT;
+      const int jobs = rem * QG * CG;
+      for (int job = tid; job < jobs; job += nt) {
+        const int t = job / (QG * CG);
+        const int qg = (job / CG) % QG, cg = job % CG;
+        const int q0 = 4 * qg, c0 = CT * cg;
+        const int shift = q0 < gx ? 0 : 1;  // pivot rows read coefficient t, the others t + 1
+        const uint32_t* w = Tq + q0;
+        const uint32_t* x = Rc + (t + shift) * CS + c0;
+        uint64_t acc[4][CT];
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int v = 0; v < CT; ++v) acc[r][v] = 0;
+        int s = 0;
+        for (; s + FE <= m; s += FE) {
+#pragma unroll
+          for (int u = 0; u < FE; ++u) {
+            const uint4 wv = *reinterpret_cast<const uint4*>(w);
+            uint32_t xv[CT];
+            if (CT == 4) {
+              const uint4 q = *reinterpret_cast<const uint4*>(x);
+              xv[0] = q.x;
+              xv[CT > 1 ? 1 : 0] = q.y;
+              xv[CT > 2 ? 2 : 0] = q.z;
+              xv[CT > 3 ? 3 : 0] = q.w;
+            } else {
+              xv[0] = *x;
+            }
+            const uint32_t wr[4] = {wv.x, wv.y, wv.z, wv.w};
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+              for (int v = 0; v < CT; ++v) acc[r][v] = mad_wide(wr[r], xv[v], acc[r][v]);
+            w += TS;
+            x += n;
+          }
+#pragma unroll
+          for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int v = 0; v < CT; ++v) acc[r][v] = fold(acc[r][v], M);
+        }
+        for (; s < m; ++s) {
+          const uint4 wv = *reinterpret_cast<const uint4*>(w);
+          const uint32_t wr[4] = {wv.x, wv.y, wv.z, wv.w};
+#pragma unroll
+          for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int v = 0; v < CT; ++v) acc[r][v] = fold(mad_wide(wr[r], x[v], acc[r][v]), M);
+          w += TS;
+          x += n;
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const int row = slotrow[q0 + r];
+          if (row >= 0) {
+            uint32_t* dst = Rn + t * CS + row * n + c0;
+#pragma unroll
+            for (int v = 0; v < CT; ++v) dst[v] = redc(acc[r][v], M);
+          }
+        }
+      }
+    }
+    __syncthreads();
+    uint32_t* tr = Rc;
+    Rc = Rn;
+    Rn = tr;
+  }
+  for (int i = tid; i < m; i += nt) {
+    P.sigma_inv[i] = inv_fermat(sigma[i], M);
+    P.delta[i] = sdelta[i];
+  }
+}
+
+// ---------------------------------------------------------------- leaves, tensor-core path (b <= 16)
+// For m <= 32 rows and n <= 16 columns the residual update runs on the int8
+// tensor cores, exactly: residues are < 2^31, so with byte limbs
+//   (T R)[i][c] = sum over a, b of 256^(a+b) (T_a R_b)[i][c],
+// and per shift class s = a + b the limb products summed over the 32-long
+// inner dimension stay below 4 * 32 * 255^2 < 2^23, exact in int32
+// (mma.sync m16n8k32 u8).  Classes 0..3 are recombined exactly in 64 bits
+// (< 2^48), classes 4..6 are added with weights 2^(8s) mod p, and one
+// Montgomery reduction gives (T R) R^{-1} -- the value the CUDA-core path
+// produces.  The residual lives in shared memory only as byte planes,
+// plane[t][limb][c][i] (one 32-byte row per column c, K index i), so each B
+// fragment is two 32-bit loads; the transform T is staged the same way for
+// the A fragments.  Row r of a plane keeps word w at w ^ 4 (r >> 2 & 1), so the
+// fragment loads of rows r and r + 4 fall in different banks.
+//
+// The elimination runs in one warp with one row per lane held in registers;
+// every column of the 48 is updated unconditionally (padding columns are
+// zero and stay zero), so the 48 updates of a step are independent.
+constexpr int kMmaRows = 32;
+constexpr int kMmaCols = 16;
+constexpr int kElimWarps = 4;         // one per SM sub-partition
+constexpr int kRpartStride = kMmaCols + 1;            // row stride of the published columns
+constexpr int kRpartSize = kMmaRows * kRpartStride;
+constexpr int kElimColsPerWarp = 12;  // 4 x 12 = 48 >= n + m
+
+// Named barrier of the elimination warps (the others wait at __syncthreads).
+__device__ __forceinline__ void elim_bar() { asm volatile("bar.sync 1, %0;" ::"n"(kElimWarps * 32) : "memory"); }
+
+__device__ __forceinline__ void leaf_mma_u8(int (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k32.row.col.s32.u8.u8.s32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+      : "+r"(d[0]), "+r"(d[1]), "+r"(d[2]), "+r"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__host__ __device__ constexpr int plane_word(int r, int w) { return r * 8 + (w ^ (((r >> 2) & 1) << 2)); }
+
+// Words of one residual coefficient in plane form: 4 limbs x (n padded to 8) rows x 8 words.
+__host__ __device__ constexpr int leaf_plane_words(int n) { return 32 * 8 * ((n + 7) / 8); }
+
+// Shared-memory bytes of pm_leaves_mma_kernel.
+size_t leaves_mma_smem_bytes(int m, int n, int K) {
+  size_t words = (size_t)2 * K * leaf_plane_words(n) + 1024 + (size_t)m * (m + 1) + (size_t)m * n + 2 * (size_t)m;
+  size_t bytes = (words * 4 + 15) & ~(size_t)15;
+  bytes += 2 * (size_t)m * 8 + (size_t)m * 4 + 64;
+  return bytes;
+}
+
+__device__ __forceinline__ void plane_store(uint32_t* coeff, int NPc, int col, int row, uint32_t v) {
+  unsigned char* b = reinterpret_cast<unsigned char*>(coeff);
+  const int wo = plane_word(col, row >> 2), bo = row & 3;
+#pragma unroll
+  for (int l = 0; l < 4; ++l) b[4 * (l * NPc * 8 + wo) + bo] = (unsigned char)(v >> (8 * l));
+}
+
+__global__ void __launch_bounds__(kLeafThreads) pm_leaves_mma_kernel(LeafParams P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int m = P.m, n = P.n, K = P.K;
+  const int W = n + m;
+  const int NT = (n + 7) / 8, MT = (m + 15) / 16, NPc = 8 * NT;
+  const int PW = leaf_plane_words(n);
+  const int TQS = m + 1;
+  const ModP M = P.M;
+  const uint32_t p = M.p;
+  uint32_t* Rc = reinterpret_cast<uint32_t*>(smem_raw);  // [K][PW] residual byte planes
+  uint32_t* Rn = Rc + K * PW;
+  uint32_t* Tp = Rn + K * PW;                             // [4][32 rows][8 words] byte planes of T
+  uint32_t* Tq = Tp + 1024;                               // [m][TQS]: Tq[s][i] = T[i][s]
+  uint32_t* R0 = Tq + m * TQS;                            // [m][n]: coefficient 0 of the residual
+  uint32_t* sigma = R0 + m * n;                           // m
+  uint32_t* sig_tmp = sigma + m;                          // m
+  const size_t w32 = (size_t)2 * K * PW + 1024 + (size_t)m * TQS + (size_t)m * n + 2 * (size_t)m;
+  int64_t* sdelta = reinterpret_cast<int64_t*>(smem_raw + ((w32 * 4 + 15) & ~(size_t)15));
+  int64_t* sdelta_tmp = sdelta + m;
+  int* perm = reinterpret_cast<int*>(sdelta_tmp + m);
+  __shared__ unsigned long long s_mx;
+  __shared__ uint32_t rpart[2 * kRpartSize];  // first n columns of A, all rows, double buffered
+
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t4 = lane & 3;
+  const uint32_t Wt[3] = {M.c32, (uint32_t)((uint64_t)M.c32 * 256 % p), (uint32_t)((uint64_t)M.c32 * 65536 % p)};
+
+  // padding bytes (rows i >= m of every column, columns c >= n) stay zero for good
+  for (int e = tid; e < 2 * K * PW + 1024; e += nt) Rc[e] = 0;
+  __syncthreads();
+  for (int e = tid; e < K * m * n; e += nt) {
+    const int t = e / (m * n), i = (e / n) % m, c = e % n;
+    const uint32_t v = P.G[(int64_t)i * P.g_rs + (int64_t)c * P.g_cs + t];
+    plane_store(Rc + t * PW, NPc, c, i, v);
+    if (t == 0) R0[i * n + c] = v;
+  }
+  for (int i = tid; i < m; i += nt) {
+    sdelta[i] = P.delta[i];
+    sigma[i] = 1;
+  }
+  __syncthreads();
+
+  for (int leaf = 0; leaf < K; ++leaf) {
+    if (warp < kElimWarps) {
+      // stable sort of delta, descending (src/sigma_basis.rs:357-359): lane q
+      // takes the row of sorted position q
+      if (warp == 0 && lane < m) {
+        const int64_t di = sdelta[lane];
+        int pos = 0;
+        for (int j = 0; j < m; ++j) {
+          const int64_t dj = sdelta[j];
+          pos += (dj > di) || (dj == di && j < lane);
+        }
+        perm[pos] = lane;
+      }
+      elim_bar();
+      const int myrow = lane < m ? perm[lane] : 0;
+      // this warp's 12 columns of row `lane` of A = [pi r | pi] (src/sigma_basis.rs:369-380)
+      const int c0 = kElimColsPerWarp * warp;
+      uint32_t a[kElimColsPerWarp];
+#pragma unroll
+      for (int cl = 0; cl < kElimColsPerWarp; ++cl) {
+        const int c = c0 + cl;
+        uint32_t v = 0;
+        if (lane < m && c < W) v = c < n ? R0[myrow * n + c] : ((c - n) == myrow ? 1u : 0u);
+        a[cl] = v;
+      }
+      // LSP elimination (src/modular_linalg.rs:188-239), fraction-free:
+      // row_i <- (piv row_i - a_i,cs row_k) R^{-1}.  Every warp keeps the list
+      // positions of the unpivoted columns (lane c < n; -1 once pivoted) and
+      // picks the non-zero column of least position.  The owners of the first
+      // n columns publish them for all rows after every update (double
+      // buffered), so one barrier per pivot step lets each warp read both row
+      // k and the pivot column.
+      int lpos = lane < n ? lane : -1;
+      int rank = 0, cur = 0;
+      bool piv_row = false;
+      auto publish = [&](uint32_t* dst) {
+        if (lane < m) {
+#pragma unroll
+          for (int cl = 0; cl < kElimColsPerWarp; ++cl)
+            if (c0 + cl < n) dst[lane * kRpartStride + c0 + cl] = a[cl];
+        }
+      };
+      publish(rpart);
+      elim_bar();
+      for (int k = 0; k < m && rank < n; ++k) {
+        const uint32_t* rp = rpart + cur * kRpartSize;
+        const uint32_t mine = lane < n ? rp[k * kRpartStride + lane] : 0u;
+        const int key = (lpos >= 0 && mine != 0) ? ((lpos << 5) | lane) : 0x7fffffff;
+        const int best = __reduce_min_sync(0xffffffffu, key);
+        if (best == 0x7fffffff) continue;  // no pivot in row k (same decision in every warp)
+        const int cs = best & 31, ts = best >> 5;
+        if (lpos >= 0) lpos = (lane == cs) ? -1 : (lpos == 0 ? ts - 1 : lpos - 1);
+        ++rank;
+        piv_row = piv_row || (lane == k);
+        const uint32_t f = lane < m ? rp[lane * kRpartStride + cs] : 0u;
+        const uint32_t piv = rp[k * kRpartStride + cs];
+        const uint32_t nf = p - f;
+        const bool upd = lane > k && lane < m;
+#pragma unroll
+        for (int cl = 0; cl < kElimColsPerWarp; ++cl) {
+          const uint32_t ak = __shfl_sync(0xffffffffu, a[cl], k);
+          const uint32_t nv = redc_2mac(piv, a[cl], nf, ak, M);
+          a[cl] = upd ? nv : a[cl];
+        }
+        if (rank < n) {  // the last pivot's update is final: nobody reads it back
+          cur ^= 1;
+          publish(rpart + cur * kRpartSize);
+          elim_bar();
+        }
+      }
+      // T (transposed) = columns n.. of A; c_i = T[i][perm[i]] (owned by one warp)
+      uint32_t* Tg = P.Tt + (size_t)leaf * m * m;
+#pragma unroll
+      for (int cl = 0; cl < kElimColsPerWarp; ++cl) {
+        const int c = c0 + cl;
+        if (c >= n && c < W && lane < m) {
+          const int s = c - n;
+          Tq[s * TQS + lane] = a[cl];
+          Tg[s * m + lane] = a[cl];
+          if (s == myrow) {
+            if (a[cl] == 0) atomicExch(P.status, 2);
+            sig_tmp[lane] = redc((uint64_t)a[cl] * sigma[myrow], M);
+          }
+        }
+      }
+      if (warp == 0) {
+        const unsigned long long mx = (unsigned long long)__ballot_sync(0xffffffffu, piv_row && lane < m);
+        if (lane < m) sdelta_tmp[lane] = sdelta[myrow] - (piv_row ? 1 : 0);  // src/sigma_basis.rs:408-411
+        if (lane == 0) {
+          P.mask[leaf] = mx;
+          s_mx = mx;
+        }
+      }
+      elim_bar();
+      if (warp == 0 && lane < m) {
+        sigma[lane] = sig_tmp[lane];
+        sdelta[lane] = sdelta_tmp[lane];
+      }
+    }
+    __syncthreads();
+    const int rem = K - leaf - 1;
+    if (rem == 0) break;
+    // byte planes of T: row i, word w holds limb l of T[i][4w .. 4w+3]
+    for (int e = tid; e < m * 8; e += nt) {
+      const int i = e >> 3, w = e & 7;
+      uint32_t v[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) v[j] = (4 * w + j < m) ? Tq[(4 * w + j) * TQS + i] : 0u;
+#pragma unroll
+      for (int l = 0; l < 4; ++l) {
+        const uint32_t lo = __byte_perm(v[0], v[1], 0x40 + 0x11 * l) & 0xffffu;  // byte l of v0, byte l of v1
+        const uint32_t hi = __byte_perm(v[2], v[3], 0x40 + 0x11 * l) & 0xffffu;
+        Tp[l * 256 + plane_word(i, w)] = lo | (hi << 16);
+      }
+    }
+    __syncthreads();
+    // residual: Rn[t][i] = T_i . Rc[t + 1 - mask_i] for t < rem, from the
+    // products P[t'] = T Rc[t'] (t' <= rem); tile (t', mt, nt) per warp
+    const unsigned long long mx = s_mx;
+    const int tiles = MT * NT;  // 1, 2 or 4: a divisor of the warp count
+    const int tile = warp % tiles, tq0 = warp / tiles, tqs = kLeafWarps / tiles;
+    const int mt = tile / NT, ntl = tile % NT;
+    const int r0 = mt * 16 + g, r1 = r0 + 8, col = ntl * 8 + g;
+    uint32_t A[4][4];
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+      A[l][0] = Tp[l * 256 + plane_word(r0, t4)];
+      A[l][1] = Tp[l * 256 + plane_word(r1, t4)];
+      A[l][2] = Tp[l * 256 + plane_word(r0, t4 + 4)];
+      A[l][3] = Tp[l * 256 + plane_word(r1, t4 + 4)];
+    }
+    for (int tq = tq0; tq <= rem; tq += tqs) {
+      uint32_t Bf[4][2];
+      const uint32_t* rc = Rc + tq * PW;
+#pragma unroll
+      for (int l = 0; l < 4; ++l) {
+        Bf[l][0] = rc[l * NPc * 8 + plane_word(col, t4)];
+        Bf[l][1] = rc[l * NPc * 8 + plane_word(col, t4 + 4)];
+      }
+      int C[7][4];
+#pragma unroll
+      for (int s = 0; s < 7; ++s)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) C[s][v] = 0;
+#pragma unroll
+      for (int l = 0; l < 4; ++l)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) leaf_mma_u8(C[l + r], A[l], Bf[r][0], Bf[r][1]);
+      // classes 0..3 exactly in 64 bits (< 2^48), classes 4..6 with their weights
+      uint32_t lo[4], hi[4];
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const uint64_t x = (uint64_t)(uint32_t)C[0][v] + ((uint64_t)(uint32_t)C[1][v] << 8) +
+                           ((uint64_t)(uint32_t)C[2][v] << 16) + ((uint64_t)(uint32_t)C[3][v] << 24);
+        lo[v] = (uint32_t)x;
+        hi[v] = (uint32_t)(x >> 32);
+        mac_cc((uint32_t)C[4][v], Wt[0], lo[v], hi[v]);
+        mac_cc((uint32_t)C[5][v], Wt[1], lo[v], hi[v]);
+        mac_cc((uint32_t)C[6][v], Wt[2], lo[v], hi[v]);
+      }
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const int row = (v < 2) ? r0 : r1;
+        const int c = ntl * 8 + 2 * t4 + (v & 1);
+        if (row < m && c < n) {
+          const int t = tq - 1 + (int)((mx >> row) & 1ull);
+          if (t >= 0 && t < rem) {
+            const uint32_t val = redc_cc(lo[v], hi[v], M);
+            plane_store(Rn + t * PW, NPc, c, row, val);
+            if (t == 0) R0[row * n + c] = val;
+          }
+        }
+      }
+    }
+    __syncthreads();
+    uint32_t* tr = Rc;
+    Rc = Rn;
+    Rn = tr;
+  }
+  for (int i = tid; i < m; i += nt) {
+    P.sigma_inv[i] = inv_fermat(sigma[i], M);
+    P.delta[i] = sdelta[i];
+  }
+}
+
+// Block basis, one CTA per column j: V_0 = e_j, V_{k+1}[t][i] = T_k[i] . V_k[t - mask_k(i)]
+// (t <= k + 1), with the same Montgomery convention as the residual; then
+// Mout[i][j][t] = V_K[t][i] sigma_inv[i].  Rows are taken in the grouped slot
+// order of the leaves kernel, four per thread, so the four rows of a thread
+// read one source coefficient.
+template <int FE>
+__global__ void __launch_bounds__(256) pm_block_basis_kernel(const uint32_t* __restrict__ Tt,
+                                                             const unsigned long long* __restrict__ mask,
+                                                             const uint32_t* __restrict__ sigma_inv, int m, int K,
+                                                             uint32_t* Mout, int64_t out_rs, int64_t out_cs, ModP M) {
+  extern __shared__ __align__(16) uint32_t bb_smem[];
+  const int S = m + 1;            // row stride of V
+  const int TS = leaf_tstride(m); // row stride of the slot-ordered transform
+  const int VS = ((K + 1) * S + 3) & ~3;  // words per V buffer (16-byte multiple)
+  uint32_t* Vc = bb_smem;                  // [K+1][S]
+  uint32_t* Vn = Vc + VS;                  // [K+1][S]
+  uint32_t* Ts = Vn + VS;                  // [m][TS], Ts[s][slot]
+  int* srow = reinterpret_cast<int*>(Ts + m * TS);  // [TS]
+  const int j = blockIdx.x;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int e = tid; e < (K + 1) * S; e += nt) Vc[e] = (e == j) ? 1u : 0u;
+  for (int k = 0; k < K; ++k) {
+    const unsigned long long mk = mask[k];
+    const int nx = __popcll(mk);
+    const int gx = (nx + 3) & ~3, QG = (gx + ((m - nx + 3) & ~3)) / 4;
+    const uint32_t* Tk = Tt + (size_t)k * m * m;
+    for (int q = tid; q < TS; q += nt) srow[q] = -1;
+    __syncthreads();
+    for (int i = tid; i < m; i += nt) srow[leaf_slot(mk, i, m)] = i;
+    __syncthreads();
+    for (int e = tid; e < m * TS; e += nt) {
+      const int s = e / TS, q = e % TS;
+      const int r = srow[q];
+      Ts[e] = r >= 0 ? Tk[s * m + r] : 0u;
+    }
+    __syncthreads();
+    const int jobs = (k + 2) * QG;
+    for (int job = tid; job < jobs; job += nt) {
+      const int t = job / QG, q0 = 4 * (job % QG);
+      const int st = t - (q0 < gx ? 1 : 0);
+      uint64_t acc[4] = {0, 0, 0, 0};
+      if (st >= 0 && st <= k) {
+        const uint32_t* w = Ts + q0;
+        const uint32_t* x = Vc + st * S;
+        int s = 0;
+        for (; s + FE <= m; s += FE) {
+#pragma unroll
+          for (int u = 0; u < FE; ++u) {
+            const uint4 wv = *reinterpret_cast<const uint4*>(w);
+            const uint32_t xv = x[s + u];
+            acc[0] = mad_wide(wv.x, xv, acc[0]);
+            acc[1] = mad_wide(wv.y, xv, acc[1]);
+            acc[2] = mad_wide(wv.z, xv, acc[2]);
+            acc[3] = mad_wide(wv.w, xv, acc[3]);
+            w += TS;
+          }
+#pragma unroll
+          for (int r = 0; r < 4; ++r) acc[r] = fold(acc[r], M);
+        }
+        for (; s < m; ++s) {
+          const uint4 wv = *reinterpret_cast<const uint4*>(w);
+          const uint32_t xv = x[s];
+          acc[0] = fold(mad_wide(wv.x, xv, acc[0]), M);
+          acc[1] = fold(mad_wide(wv.y, xv, acc[1]), M);
+          acc[2] = fold(mad_wide(wv.z, xv, acc[2]), M);
+          acc[3] = fold(mad_wide(wv.w, xv, acc[3]), M);
+          w += TS;
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int row = srow[q0 + r];
+        if (row >= 0) Vn[t * S + row] = (st >= 0 && st <= k) ? redc(acc[r], M) : 0u;
+      }
+    }
+    __syncthreads();
+    uint32_t* tv = Vc;
+    Vc = Vn;
+    Vn = tv;
+  }
+  for (int e = tid; e < (K + 1) * m; e += nt) {
+    const int t = e / m, r = e % m;
+    Mout[(int64_t)r * out_rs + (int64_t)j * out_cs + t] = mulmod(Vc[t * S + r], sigma_inv[r], M);
+  }
+}
+
 // ---------------------------------------------------------------- host side
 uint32_t find_generator(uint32_t p) {
   std::vector<uint32_t> fac;
@@ -526,10 +1196,14 @@ struct Pm {
   int64_t nmax = 0;
   DevBuf<uint32_t> tw, tws, twi, twis;
   DevBuf<uint32_t> FA, FB, FC;
-  DevBuf<uint32_t> Mbuf;
+  DevBuf<uint32_t> Tt;                 // leaf transforms of one block [K][m][m]
+  DevBuf<unsigned long long> leafmask; // [K]
+  DevBuf<uint32_t> sigma_inv;          // [m]
   DevBuf<int64_t> delta;
   DevBuf<int> status;
-  size_t base_smem = 0;
+  int64_t cs = 0;                      // residual coefficient stride of the leaves kernel (words)
+  int fold4 = 0;
+  bool mma = false;                    // tensor-core leaves kernel (b <= 16)
   // per recursion depth: MM, GG, MMM
   std::vector<std::unique_ptr<DevBuf<uint32_t>>> bufs;
   Twiddles fwd() const { return Twiddles{tw.ptr, tws.ptr, nmax}; }
@@ -604,34 +1278,69 @@ int poly_mat_mul(Pm& P, const uint32_t* A, int mA, int r, int64_t la, int64_t a_
 
 int run_base(Pm& P, const uint32_t* G, int64_t g_rs, int64_t g_cs, int nleaves, uint32_t* Mout, int64_t o_rs,
              int64_t o_cs) {
-  BaseParams B;
-  B.G = G;
-  B.g_rs = g_rs;
-  B.g_cs = g_cs;
-  B.m = P.m;
-  B.n = P.n;
-  B.nleaves = nleaves;
-  B.delta = P.delta.ptr;
-  B.Mout = Mout;
-  B.out_rs = o_rs;
-  B.out_cs = o_cs;
-  B.Mbuf = P.Mbuf.ptr;
-  B.m_smem = 1;
-  B.M = P.M;
-  B.status = P.status.ptr;
-  if (P.n % 4 == 0) pm_base_kernel<4><<<1, kBaseThreads, P.base_smem, P.s>>>(B);
-  else pm_base_kernel<1><<<1, kBaseThreads, P.base_smem, P.s>>>(B);
+  LeafParams L;
+  L.G = G;
+  L.g_rs = g_rs;
+  L.g_cs = g_cs;
+  L.m = P.m;
+  L.n = P.n;
+  L.K = nleaves;
+  L.cs = P.cs;
+  L.delta = P.delta.ptr;
+  L.Tt = P.Tt.ptr;
+  L.mask = P.leafmask.ptr;
+  L.sigma_inv = P.sigma_inv.ptr;
+  L.M = P.M;
+  L.status = P.status.ptr;
+  if (P.mma) {
+    pm_leaves_mma_kernel<<<1, kLeafThreads, leaves_mma_smem_bytes(P.m, P.n, nleaves), P.s>>>(L);
+  } else if (P.n % 4 == 0) {
+    const size_t smem = leaves_smem_bytes(P.m, P.n, nleaves, P.cs);
+    if (P.fold4) pm_leaves_kernel<4, 4><<<1, kLeafThreads, smem, P.s>>>(L);
+    else pm_leaves_kernel<4, 2><<<1, kLeafThreads, smem, P.s>>>(L);
+  } else {
+    const size_t smem = leaves_smem_bytes(P.m, P.n, nleaves, P.cs);
+    if (P.fold4) pm_leaves_kernel<1, 4><<<1, kLeafThreads, smem, P.s>>>(L);
+    else pm_leaves_kernel<1, 2><<<1, kLeafThreads, smem, P.s>>>(L);
+  }
+  RR_CUDA(cudaGetLastError());
+  const size_t bsm = block_basis_smem_bytes(P.m, nleaves);
+  if (P.fold4)
+    pm_block_basis_kernel<4><<<P.m, 256, bsm, P.s>>>(P.Tt.ptr, P.leafmask.ptr, P.sigma_inv.ptr, P.m, nleaves, Mout,
+                                                     o_rs, o_cs, P.M);
+  else
+    pm_block_basis_kernel<2><<<P.m, 256, bsm, P.s>>>(P.Tt.ptr, P.leafmask.ptr, P.sigma_inv.ptr, P.m, nleaves, Mout,
+                                                     o_rs, o_cs, P.M);
   RR_CUDA(cudaGetLastError());
   return RR_OK;
 }
 
-// Largest block of leaves (a power of two <= 32 and <= d) whose residual and
-// basis fit in shared memory.
-int pick_block_leaves(int m, int n, int64_t d, size_t* smem) {
-  int K = (int)std::min<int64_t>(d, 32);
-  while (K > 1 && base_smem_bytes(m, n, K, true) > kBaseSmemBudget) K /= 2;
-  *smem = base_smem_bytes(m, n, K, true);
+// Residual coefficient stride of the leaves kernel: m * n rounded to 16-byte
+// words plus 4, so that neighbouring coefficients start in different banks.
+int64_t leaf_coeff_stride(int m, int n) { return (((int64_t)m * n + 3) & ~(int64_t)3) + 4; }
+
+// Largest block of leaves (a power of two <= 64 for m <= 16, <= 32 otherwise,
+// and <= d) whose double-buffered residual fits in shared memory.
+int pick_block_leaves(int m, int n, int64_t d, bool mma, size_t* smem) {
+  const int kmax = m <= 16 ? 64 : 32;
+  int K = (int)std::min<int64_t>(d, kmax);
+  const int64_t cs = leaf_coeff_stride(m, n);
+  auto bytes = [&](int k) { return mma ? leaves_mma_smem_bytes(m, n, k) : leaves_smem_bytes(m, n, k, cs); };
+  while (K > 1 && bytes(K) > kBaseSmemBudget) K /= 2;
+  *smem = bytes(K);
   return K;
+}
+
+int set_leaves_smem_limit(size_t bytes, size_t basis_bytes) {
+  const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  RR_CUDA(cudaFuncSetAttribute(pm_leaves_kernel<4, 4>, attr, (int)bytes));
+  RR_CUDA(cudaFuncSetAttribute(pm_leaves_kernel<4, 2>, attr, (int)bytes));
+  RR_CUDA(cudaFuncSetAttribute(pm_leaves_kernel<1, 4>, attr, (int)bytes));
+  RR_CUDA(cudaFuncSetAttribute(pm_leaves_kernel<1, 2>, attr, (int)bytes));
+  RR_CUDA(cudaFuncSetAttribute(pm_leaves_mma_kernel, attr, (int)bytes));
+  RR_CUDA(cudaFuncSetAttribute(pm_block_basis_kernel<4>, attr, (int)basis_bytes));
+  RR_CUDA(cudaFuncSetAttribute(pm_block_basis_kernel<2>, attr, (int)basis_bytes));
+  return RR_OK;
 }
 
 int set_base_smem_limit(size_t bytes) {
@@ -670,7 +1379,16 @@ int pm_basis_device(rr_ctx* ctx, const uint32_t* seq, int64_t seq_stride, int b,
   P.n = b;
   P.p = p;
   P.M = make_modp(p);
-  P.K = pick_block_leaves(P.m, P.n, d, &P.base_smem);
+  size_t leaves_smem = 0;
+  P.mma = P.m <= kMmaRows && P.n <= kMmaCols;
+  P.K = pick_block_leaves(P.m, P.n, d, P.mma, &leaves_smem);
+  P.cs = leaf_coeff_stride(P.m, P.n);
+  {
+    // four products fit between folds iff (2^32-1)*c32 + 2^32 - 1 + 4 (p-1)^2 < 2^64
+    const unsigned __int128 F = (unsigned __int128)0xffffffffull * P.M.c32 + 0xffffffffull;
+    const unsigned __int128 q = (unsigned __int128)(p - 1) * (p - 1);
+    P.fold4 = (F + 4 * q) < ((unsigned __int128)1 << 64);
+  }
   const int m = P.m, n = P.n;
   // NTT table for the largest product: length nextpow2(3d/2 + 1) = 2d (d >= 2)
   int64_t nmax = 1;
@@ -720,9 +1438,16 @@ int pm_basis_device(rr_ctx* ctx, const uint32_t* seq, int64_t seq_stride, int b,
   }
   RR_TRY(P.delta.alloc_async(m, P.s));
   RR_TRY(P.status.alloc_async(1, P.s));
+  RR_TRY(P.Tt.alloc_async((size_t)P.K * m * m, P.s));
+  RR_TRY(P.leafmask.alloc_async((size_t)P.K, P.s));
+  RR_TRY(P.sigma_inv.alloc_async((size_t)m, P.s));
   RR_CUDA(cudaMemsetAsync(P.delta.ptr, 0, m * sizeof(int64_t), P.s));
   RR_CUDA(cudaMemsetAsync(P.status.ptr, 0, sizeof(int), P.s));
-  RR_TRY(set_base_smem_limit(P.base_smem));
+  // the limits are per kernel, shared by every caller in the process (the
+  // batched engine runs generators on several threads): always the budget,
+  // never this call's size, so a concurrent smaller call cannot lower them
+  if (leaves_smem > kBaseSmemBudget) return fail(RR_EUNSUPPORTED, "leaf block needs %zu bytes of shared memory", leaves_smem);
+  RR_TRY(set_leaves_smem_limit(kBaseSmemBudget, block_basis_smem_bytes(64, 64)));
   // G = [S; I], coefficients [0, d]
   DevBuf<uint32_t> dseq, G;
   const int np = b * (b + 1) / 2;
