@@ -184,6 +184,41 @@ int rr_batch_ranks(rr_batch* batch, int32_t workers, int64_t* ranks);
 int rr_batch_info(const rr_batch* batch, int64_t* total_rows, int64_t* total_cols, int64_t* total_nnz,
                   int64_t* max_apps);
 
+/* ---------------------------------------------------------------- serving */
+/* A rank service: requests (one matrix each, with its preconditioners and V)
+ * are submitted as they arrive and run concurrently.  A request is admitted
+ * when its device footprint fits hbm_budget and fewer than max_active
+ * requests are resident; its matrix and Krylov state stay on the device while
+ * the scheduler interleaves chunks of chunk_apps applications of B of all
+ * running requests over `lanes` streams; when its sequence is complete a
+ * worker thread solves the generator and reads off the rank, and its memory
+ * admits the next requests.  Each request gets exactly the rank rr_rank
+ * gives on the same inputs.  The reference has no service: it ranks one
+ * matrix per run of src/main.rs:254-639 (commands.txt). */
+typedef struct rr_server_s rr_server;
+typedef struct rr_server_config {
+  int32_t b;           /* block width of every request */
+  uint32_t p;          /* prime */
+  int32_t lanes;       /* Krylov streams (0: 4) */
+  int32_t workers;     /* loader / generator threads (0: 4) */
+  int32_t max_active;  /* requests resident at once (0: 64) */
+  int64_t chunk_apps;  /* applications of B per scheduling quantum (0: 64) */
+  uint64_t hbm_budget; /* device bytes the resident requests may hold (0: 80% of free memory) */
+} rr_server_config;
+int rr_server_create(int device, const rr_server_config* cfg, rr_server** out);
+/* Copies the request; *id identifies it.  RR_ENOMEM when it alone exceeds the budget. */
+int rr_server_submit(rr_server* server, int64_t m, int64_t n, const int64_t* rowptr, const int32_t* col,
+                     const uint32_t* val, const uint32_t* row_precond, const uint32_t* col_precond, const uint32_t* V,
+                     uint64_t* id);
+/* Waits for request id (timeout_s < 0: no limit; RR_ETIMEOUT when it runs out);
+ * *rank as rr_rank, *latency_ms = submit to completion (may be NULL). */
+int rr_server_wait(rr_server* server, uint64_t id, double timeout_s, int64_t* rank, double* latency_ms);
+/* Requests submitted and completed, latency percentiles of the completed
+ * ones and completions per second between the first submit and the last completion. */
+int rr_server_stats(rr_server* server, int64_t* submitted, int64_t* completed, double* p50_ms, double* p99_ms,
+                    double* ranks_per_s);
+int rr_server_destroy(rr_server* server);
+
 /* ---------------------------------------------------------------- files */
 /* .wdm checkpoint (src/wdm_files.rs:10-19): header "m n p Nlen num_v", then
  * row_precond, col_precond, num_v lines of v, num_v lines of curv and

@@ -47,7 +47,7 @@ def _close_all():
 
 __all__ = ["Context", "CsrMatrix", "DeviceMatrix", "KrylovStream", "main_loop_s_mt2", "PM_Basis",
            "analyze_pm_basis", "block_wiedemann_rank", "save_wdm_file_sym", "load_wdm_file_sym",
-           "default_max_nlen", "RRError"]
+           "default_max_nlen", "Batch", "Server", "RRError"]
 
 DEFAULT_PRIME = 2013265921
 
@@ -379,6 +379,64 @@ class Batch:
     def close(self):
         if getattr(self, "handle", None):
             lib().rr_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Rank service (rr_server_*): requests are submitted as they arrive,
+    admitted by device-memory footprint, their Krylov steps interleaved on
+    several streams and their generators solved by worker threads.  Every
+    request gets exactly the rank :func:`block_wiedemann_rank` gives on the
+    same inputs."""
+
+    def __init__(self, num_v: int, theprime: int = DEFAULT_PRIME, lanes: int = 4, workers: int = 4,
+                 max_active: int = 64, chunk_apps: int = 64, hbm_budget: int = 0, device: int = 0):
+        from ._lib import ServerConfig
+
+        cfg = ServerConfig(int(num_v), int(theprime), int(lanes), int(workers), int(max_active), int(chunk_apps),
+                           int(hbm_budget))
+        h = C.c_void_p()
+        check(lib().rr_server_create(device, C.byref(cfg), C.byref(h)))
+        self.handle = h
+        self.b = int(num_v)
+        _track(self, 0)
+
+    def submit(self, rowptr, col, val, m: int, n: int, row_precond, col_precond, v) -> int:
+        rowptr = np.ascontiguousarray(rowptr, np.int64)
+        col = np.ascontiguousarray(col, np.int32)
+        val = np.ascontiguousarray(val, np.uint32)
+        rp = np.ascontiguousarray(row_precond, np.uint32)
+        cp = np.ascontiguousarray(col_precond, np.uint32)
+        v = np.ascontiguousarray(v, np.uint32)
+        if rp.size != m or cp.size != n or v.shape != (self.b, n):
+            raise ValueError("preconditioner or block shapes do not match the matrix")
+        rid = C.c_uint64()
+        check(lib().rr_server_submit(self.handle, m, n, ptr(rowptr), ptr(col), ptr(val), ptr(rp), ptr(cp), ptr(v),
+                                     C.byref(rid)))
+        return rid.value
+
+    def result(self, rid: int, timeout: float = -1.0):
+        """(rank, latency in ms) of request ``rid``, waiting up to ``timeout`` seconds (< 0: no limit)."""
+        r, lat = C.c_int64(), C.c_double()
+        check(lib().rr_server_wait(self.handle, rid, float(timeout), C.byref(r), C.byref(lat)))
+        return r.value, lat.value
+
+    def stats(self):
+        a, b = C.c_int64(), C.c_int64()
+        p50, p99, rps = C.c_double(), C.c_double(), C.c_double()
+        check(lib().rr_server_stats(self.handle, C.byref(a), C.byref(b), C.byref(p50), C.byref(p99), C.byref(rps)))
+        return {"submitted": a.value, "completed": b.value, "p50_ms": p50.value, "p99_ms": p99.value,
+                "ranks_per_s": rps.value}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().rr_server_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

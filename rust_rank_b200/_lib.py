@@ -58,7 +58,20 @@ SIGNATURES = {
     "rr_wdm_save": (C.c_int, [C.c_char_p, _i64, _i64, _u32, _i32, _vp, _vp, _vp, _vp, _vp, _i64, _i64]),
     "rr_wdm_load": (C.c_int, [C.c_char_p, _pi64, _pi64, _pu32, _pi32, _pi64, _vp, _vp, _vp, _vp, _vp, _i64]),
     "rr_sms_load": (C.c_int, [C.c_char_p, _u32, _pi64, _pi64, _pi64, _vp, _vp, _vp]),
+    "rr_server_create": (C.c_int, [C.c_int, _vp, C.POINTER(_vp)]),
+    "rr_server_submit": (C.c_int, [_vp, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp, C.POINTER(C.c_uint64)]),
+    "rr_server_wait": (C.c_int, [_vp, C.c_uint64, C.c_double, _pi64, C.POINTER(C.c_double)]),
+    "rr_server_stats": (C.c_int, [_vp, _pi64, _pi64, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                  C.POINTER(C.c_double)]),
+    "rr_server_destroy": (C.c_int, [_vp]),
 }
+
+
+class ServerConfig(C.Structure):
+    """rr_server_config of include/rr_rank.h."""
+
+    _fields_ = [("b", C.c_int32), ("p", C.c_uint32), ("lanes", C.c_int32), ("workers", C.c_int32),
+                ("max_active", C.c_int32), ("chunk_apps", C.c_int64), ("hbm_budget", C.c_uint64)]
 
 _LIB = None
 

@@ -69,6 +69,35 @@ int launch_scatter_block(rr_krylov* kr, const uint32_t* d_V, uint32_t* d_out);
 
 using namespace rr;
 
+// ---------------------------------------------------------------- Krylov
+static int padded_width(int b) { return b <= 4 ? 4 : b <= 8 ? 8 : b <= 16 ? 16 : 32; }
+
+static int ensure_capacity(rr_krylov* kr, int64_t terms) {
+  const int np = kr->b * (kr->b + 1) / 2;
+  if (terms <= kr->cap) return RR_OK;
+  int64_t ncap = std::max<int64_t>(terms, 2 * kr->cap);
+  cudaStream_t s = kr->mat->ctx->stream;
+  DevBuf<uint32_t> nb;
+  RR_TRY(nb.alloc_async((size_t)ncap * np, s));
+  if (kr->cap > 0) RR_CUDA(cudaMemcpyAsync(nb.ptr, kr->S.ptr, (size_t)kr->cap * np * 4, cudaMemcpyDeviceToDevice, s));
+  // stream-ordered: the old buffer is freed after the copy and every queued step
+  std::swap(kr->S.ptr, nb.ptr);
+  std::swap(kr->S.n, nb.n);
+  std::swap(kr->S.stream, nb.stream);
+  std::swap(kr->S.ordered, nb.ordered);
+  kr->cap = ncap;
+  return RR_OK;
+}
+
+namespace rr {
+// Device sequence buffer sized for `terms` terms up front (no regrowth, and
+// so no stream synchronisation, while the handle is stepped).
+int krylov_reserve(rr_krylov* kr, int64_t terms) {
+  RR_CUDA(cudaSetDevice(kr->mat->ctx->device));
+  return ensure_capacity(kr, terms);
+}
+}  // namespace rr
+
 extern "C" {
 
 const char* rr_status_string(int s) {
@@ -163,8 +192,7 @@ int rr_matrix_create(rr_ctx* ctx, int64_t m, int64_t n, const int64_t* rowptr, c
 int rr_matrix_destroy(rr_matrix* mat) {
   if (!mat) return RR_OK;
   cudaSetDevice(mat->ctx->device);
-  cudaStreamSynchronize(mat->ctx->stream);
-  delete mat;
+  delete mat;  // stream-ordered frees: after the work queued on the context's stream
   return RR_OK;
 }
 
@@ -180,24 +208,6 @@ int rr_matrix_shape(const rr_matrix* mat, int64_t* m, int64_t* n, int64_t* nnz) 
   *m = mat->m;
   *n = mat->n;
   *nnz = mat->nnz;
-  return RR_OK;
-}
-
-// ---------------------------------------------------------------- Krylov
-static int padded_width(int b) { return b <= 4 ? 4 : b <= 8 ? 8 : b <= 16 ? 16 : 32; }
-
-static int ensure_capacity(rr_krylov* kr, int64_t terms) {
-  const int np = kr->b * (kr->b + 1) / 2;
-  if (terms <= kr->cap) return RR_OK;
-  int64_t ncap = std::max<int64_t>(terms, 2 * kr->cap);
-  DevBuf<uint32_t> nb;
-  RR_TRY(nb.alloc((size_t)ncap * np));
-  if (kr->cap > 0)
-    RR_CUDA(cudaMemcpyAsync(nb.ptr, kr->S.ptr, (size_t)kr->cap * np * 4, cudaMemcpyDeviceToDevice, kr->mat->ctx->stream));
-  RR_CUDA(cudaStreamSynchronize(kr->mat->ctx->stream));
-  std::swap(kr->S.ptr, nb.ptr);
-  std::swap(kr->S.n, nb.n);
-  kr->cap = ncap;
   return RR_OK;
 }
 
@@ -251,10 +261,10 @@ int rr_krylov_create(rr_matrix* mat, int32_t b, const uint32_t* row_precond, con
       dcr[i] = (uint32_t)(dc[i] * R1 % p);
       dc[i] = (uint32_t)(dc[i] * R2 % p);
     }
-    RR_TRY(kr->dr_m.alloc(m));
-    RR_TRY(kr->dc_m.alloc(n));
-    RR_TRY(kr->dc_r.alloc(n));
-    RR_TRY(kr->dcinv.alloc(n));
+    RR_TRY(kr->dr_m.alloc_async(m, s));
+    RR_TRY(kr->dc_m.alloc_async(n, s));
+    RR_TRY(kr->dc_r.alloc_async(n, s));
+    RR_TRY(kr->dcinv.alloc_async(n, s));
     RR_CUDA(cudaMemcpyAsync(kr->dr_m.ptr, dr.data(), m * 4, cudaMemcpyHostToDevice, s));
     RR_CUDA(cudaMemcpyAsync(kr->dc_m.ptr, dc.data(), n * 4, cudaMemcpyHostToDevice, s));
     RR_CUDA(cudaMemcpyAsync(kr->dc_r.ptr, dcr.data(), n * 4, cudaMemcpyHostToDevice, s));
@@ -262,15 +272,15 @@ int rr_krylov_create(rr_matrix* mat, int32_t b, const uint32_t* row_precond, con
     RR_CUDA(cudaStreamSynchronize(s));  // host vectors die at scope end
   }
   const int B = kr->B;
-  RR_TRY(kr->X[0].alloc((size_t)n * B));
-  RR_TRY(kr->X[1].alloc((size_t)n * B));
-  RR_TRY(kr->U.alloc((size_t)m * B));
+  RR_TRY(kr->X[0].alloc_async((size_t)n * B, s));
+  RR_TRY(kr->X[1].alloc_async((size_t)n * B, s));
+  RR_TRY(kr->U.alloc_async((size_t)m * B, s));
   const int64_t heavy = std::max<int64_t>(std::max(mat->A.heavy_rows, mat->At.heavy_rows), 1);
-  RR_TRY(kr->heavy_acc.alloc((size_t)heavy * B));
+  RR_TRY(kr->heavy_acc.alloc_async((size_t)heavy * B, s));
   RR_CUDA(cudaMemsetAsync(kr->heavy_acc.ptr, 0, kr->heavy_acc.bytes(), s));
-  RR_TRY(kr->gram_acc.alloc((size_t)kGramReplicas * (B * (B + 1) / 2)));
+  RR_TRY(kr->gram_acc.alloc_async((size_t)kGramReplicas * (B * (B + 1) / 2), s));
   RR_CUDA(cudaMemsetAsync(kr->gram_acc.ptr, 0, kr->gram_acc.bytes(), s));
-  RR_TRY(kr->counter.alloc(4));
+  RR_TRY(kr->counter.alloc_async(4, s));
   RR_CUDA(cudaMemsetAsync(kr->counter.ptr, 0, kr->counter.bytes(), s));
   RR_TRY(krylov_occupancy(kr.get()));
   kr->base = seq_len;
@@ -279,7 +289,7 @@ int rr_krylov_create(rr_matrix* mat, int32_t b, const uint32_t* row_precond, con
   // upload curv (vector-major), scatter into device order, x = D_c w
   {
     DevBuf<uint32_t> v;
-    RR_TRY(v.alloc((size_t)b * n));
+    RR_TRY(v.alloc_async((size_t)b * n, s));
     RR_CUDA(cudaMemcpyAsync(v.ptr, curv, (size_t)b * n * 4, cudaMemcpyHostToDevice, s));
     RR_TRY(launch_scatter_block(kr.get(), v.ptr, kr->X[1].ptr));
     kr->cur = 0;
@@ -294,8 +304,7 @@ int rr_krylov_create(rr_matrix* mat, int32_t b, const uint32_t* row_precond, con
 int rr_krylov_destroy(rr_krylov* kr) {
   if (!kr) return RR_OK;
   cudaSetDevice(kr->mat->ctx->device);
-  cudaStreamSynchronize(kr->mat->ctx->stream);
-  delete kr;
+  delete kr;  // stream-ordered frees: after the work queued on the context's stream
   return RR_OK;
 }
 
@@ -359,7 +368,7 @@ int rr_krylov_get_curv(rr_krylov* kr, uint32_t* curv) {
   if (!kr || !curv) return fail(RR_EINVAL, "NULL argument");
   RR_CUDA(cudaSetDevice(kr->mat->ctx->device));
   DevBuf<uint32_t> out;
-  RR_TRY(out.alloc((size_t)kr->b * kr->mat->n));
+  RR_TRY(out.alloc_async((size_t)kr->b * kr->mat->n, kr->mat->ctx->stream));
   RR_TRY(krylov_launch_get_curv(kr, out.ptr));
   RR_CUDA(cudaMemcpyAsync(curv, out.ptr, out.bytes(), cudaMemcpyDeviceToHost, kr->mat->ctx->stream));
   RR_CUDA(cudaStreamSynchronize(kr->mat->ctx->stream));

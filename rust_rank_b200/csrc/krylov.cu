@@ -937,8 +937,8 @@ int upload_csr(const HostCsr& h, DevCsr& d, cudaStream_t s) {
   d.rows = h.rows;
   d.cols = h.cols;
   d.nnz = (int64_t)h.cv.size();
-  RR_TRY(d.rowptr.alloc(h.ptr.size()));
-  RR_TRY(d.cv.alloc(std::max<size_t>(h.cv.size(), 1)));
+  RR_TRY(d.rowptr.alloc_async(h.ptr.size(), s));
+  RR_TRY(d.cv.alloc_async(std::max<size_t>(h.cv.size(), 1), s));
   RR_CUDA(cudaMemcpyAsync(d.rowptr.ptr, h.ptr.data(), h.ptr.size() * 4, cudaMemcpyHostToDevice, s));
   if (!h.cv.empty())
     RR_CUDA(cudaMemcpyAsync(d.cv.ptr, h.cv.data(), h.cv.size() * sizeof(uint2), cudaMemcpyHostToDevice, s));
@@ -959,9 +959,9 @@ int upload_csr(const HostCsr& h, DevCsr& d, cudaStream_t s) {
   if (d.nchunks) {
     std::vector<uint32_t> cr(d.nchunks), cb(d.nchunks), ce(d.nchunks);
     for (int64_t i = 0; i < d.nchunks; ++i) { cr[i] = chunks[i].row; cb[i] = chunks[i].beg; ce[i] = chunks[i].end; }
-    RR_TRY(d.chunk_row.alloc(d.nchunks));
-    RR_TRY(d.chunk_begin.alloc(d.nchunks));
-    RR_TRY(d.chunk_end.alloc(d.nchunks));
+    RR_TRY(d.chunk_row.alloc_async(d.nchunks, s));
+    RR_TRY(d.chunk_begin.alloc_async(d.nchunks, s));
+    RR_TRY(d.chunk_end.alloc_async(d.nchunks, s));
     RR_CUDA(cudaMemcpyAsync(d.chunk_row.ptr, cr.data(), d.nchunks * 4, cudaMemcpyHostToDevice, s));
     RR_CUDA(cudaMemcpyAsync(d.chunk_begin.ptr, cb.data(), d.nchunks * 4, cudaMemcpyHostToDevice, s));
     RR_CUDA(cudaMemcpyAsync(d.chunk_end.ptr, ce.data(), d.nchunks * 4, cudaMemcpyHostToDevice, s));
@@ -1004,7 +1004,7 @@ int matrix_build(rr_ctx* ctx, int64_t m, int64_t n, const int64_t* rowptr, const
   cudaStream_t s = ctx->stream;
   RR_TRY(upload_csr(A, mat->A, s));
   RR_TRY(upload_csr(At, mat->At, s));
-  RR_TRY(mat->d_colperm.alloc(std::max<int64_t>(n, 1)));
+  RR_TRY(mat->d_colperm.alloc_async(std::max<int64_t>(n, 1), s));
   RR_CUDA(cudaMemcpyAsync(mat->d_colperm.ptr, mat->colperm.data(), n * 4, cudaMemcpyHostToDevice, s));
   RR_CUDA(cudaStreamSynchronize(s));
   (void)p;

@@ -149,6 +149,7 @@ struct rr_krylov_s {
 
 namespace rr {
 int krylov_launch_init(rr_krylov* kr, const uint32_t* d_w, bool emit_s0);
+int krylov_reserve(rr_krylov* kr, int64_t terms);
 int krylov_launch_application(rr_krylov* kr, cudaEvent_t* ev);
 int krylov_launch_get_curv(rr_krylov* kr, uint32_t* d_out);
 int krylov_occupancy(rr_krylov* kr);
