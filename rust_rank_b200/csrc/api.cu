@@ -85,6 +85,9 @@ static int ensure_capacity(rr_krylov* kr, int64_t terms) {
   std::swap(kr->S.n, nb.n);
   std::swap(kr->S.stream, nb.stream);
   std::swap(kr->S.ordered, nb.ordered);
+  // the kernels find S through device memory (captured launches stay valid)
+  RR_CUDA(cudaMemcpyAsync(kr->d_sptr.ptr, &kr->S.ptr, sizeof(uint32_t*), cudaMemcpyHostToDevice, s));
+  RR_CUDA(cudaStreamSynchronize(s));  // the source is a host field that may change again
   kr->cap = ncap;
   return RR_OK;
 }
@@ -135,6 +138,15 @@ int rr_ctx_create(int device, rr_ctx** out) {
   RR_CUDA(cudaGetDeviceProperties(&prop, device));
   if (prop.major < 10)
     return fail(RR_EUNSUPPORTED, "device %d is sm_%d%d; this build targets sm_100a", device, prop.major, prop.minor);
+  {
+    // keep freed stream-ordered memory in this process's pool instead of
+    // returning it to the driver at every synchronisation (the generator
+    // allocates its NTT workspace per call)
+    cudaMemPool_t pool;
+    RR_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t keep = ~0ull;
+    RR_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  }
   std::unique_ptr<rr_ctx> c(new rr_ctx);
   c->device = device;
   c->num_sms = prop.multiProcessorCount;
@@ -282,6 +294,14 @@ int rr_krylov_create(rr_matrix* mat, int32_t b, const uint32_t* row_precond, con
   RR_CUDA(cudaMemsetAsync(kr->gram_acc.ptr, 0, kr->gram_acc.bytes(), s));
   RR_TRY(kr->counter.alloc_async(4, s));
   RR_CUDA(cudaMemsetAsync(kr->counter.ptr, 0, kr->counter.bytes(), s));
+  RR_TRY(kr->d_term.alloc_async(1, s));
+  RR_TRY(kr->d_sptr.alloc_async(1, s));
+  {
+    // first application's odd term: slot 1 after S_0 of a fresh start, slot 0 on resume
+    const unsigned int slot0 = seq_len == 0 ? 1u : 0u;
+    RR_CUDA(cudaMemcpyAsync(kr->d_term.ptr, &slot0, sizeof(slot0), cudaMemcpyHostToDevice, s));
+    RR_CUDA(cudaStreamSynchronize(s));
+  }
   RR_TRY(krylov_occupancy(kr.get()));
   kr->base = seq_len;
   kr->len = seq_len;
@@ -308,10 +328,55 @@ int rr_krylov_destroy(rr_krylov* kr) {
   return RR_OK;
 }
 
+// Applications per captured graph (even, so the block buffers end where they
+// started and the graph can be replayed), and the run length that uses it.
+constexpr int64_t kGraphApps = 16;
+constexpr int64_t kGraphMinRun = 2 * kGraphApps;
+
+// Captures kGraphApps applications (they are recorded, not run: the host
+// state the launches advance is restored afterwards).
+static int capture_graph(rr_krylov* kr) {
+  cudaStream_t s = kr->mat->ctx->stream;
+  const int64_t len0 = kr->len, launches0 = kr->launches;
+  const int cur0 = kr->cur;
+  RR_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  int st = RR_OK;
+  for (int64_t i = 0; i < kGraphApps && st == RR_OK; ++i) st = krylov_launch_application(kr, nullptr);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(s, &g);
+  kr->graph_launches = kr->launches - launches0;
+  kr->len = len0;
+  kr->cur = cur0;
+  kr->launches = launches0;
+  if (st != RR_OK) {
+    if (g) cudaGraphDestroy(g);
+    return st;
+  }
+  RR_CUDA(e);
+  const cudaError_t ei = cudaGraphInstantiate(&kr->graph, g, 0);
+  cudaGraphDestroy(g);
+  RR_CUDA(ei);
+  kr->graph_cur = cur0;
+  return RR_OK;
+}
+
 static int queue_apps(rr_krylov* kr, int64_t n_apps) {
   if (kr->len == 0) kr->len = 1;  // publish S_0
   RR_TRY(ensure_capacity(kr, kr->len - kr->base + 2 * n_apps + 1));
-  for (int64_t i = 0; i < n_apps; ++i) RR_TRY(krylov_launch_application(kr, nullptr));
+  int64_t i = 0;
+  if (n_apps >= kGraphMinRun) {
+    if (!kr->graph) RR_TRY(capture_graph(kr));
+    if (kr->cur != kr->graph_cur) {
+      RR_TRY(krylov_launch_application(kr, nullptr));
+      ++i;
+    }
+    for (; n_apps - i >= kGraphApps; i += kGraphApps) {
+      RR_CUDA(cudaGraphLaunch(kr->graph, kr->mat->ctx->stream));
+      kr->len += 2 * kGraphApps;
+      kr->launches += kr->graph_launches;
+    }
+  }
+  for (; i < n_apps; ++i) RR_TRY(krylov_launch_application(kr, nullptr));
   return RR_OK;
 }
 

@@ -394,7 +394,8 @@ __global__ void __launch_bounds__(kThreads, 4) pass_kernel(PassParams P) {
 
   for (int q = threadIdx.x; q < NP; q += kThreads) red[q] = 0;
   Gram gram;
-  if (P.S_out != nullptr) gram.init(gram_smem + (size_t)warp * Gram::kWords, lane);
+  const bool emit = P.S_out != nullptr || P.term_ctr != nullptr;
+  if (emit) gram.init(gram_smem + (size_t)warp * Gram::kWords, lane);
   __syncthreads();  // red[] zeroed before a warp may emit into it
 
   const int64_t nbatch = (P.rows + RPW - 1) / RPW;
@@ -429,7 +430,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass_kernel(PassParams P) {
   }
 
   for (int64_t batch = b_first; batch < b_stop; batch += b_step) {
-    if (segmented && P.S_out != nullptr) {
+    if (segmented && emit) {
       const int sg = P.batch_seg[batch];
       if (sg != cur_seg) {
         if (cur_seg >= 0) {
@@ -502,10 +503,10 @@ __global__ void __launch_bounds__(kThreads, 4) pass_kernel(PassParams P) {
 #pragma unroll
       for (int l = 0; l < LPT; ++l) { gz[l] = 0; gu[l] = 0; }
     }
-    if (P.S_out != nullptr) gram.add(gz, gu, slot, sub, lane, M, W);
+    if (emit) gram.add(gz, gu, slot, sub, lane, M, W);
   }
 
-  if (P.S_out == nullptr) return;
+  if (!emit) return;
   gram.finish(slot, sub, lane, M, W);
   __syncthreads();  // red[] is zeroed before any warp emits into it
   if (segmented) {
@@ -559,17 +560,20 @@ __global__ void __launch_bounds__(kThreads, 4) pass_kernel(PassParams P) {
       }
     }
   } else {
+    uint32_t* S_out = P.S_out;
+    if (P.term_ctr != nullptr) S_out = *P.S_ptr + (size_t)__ldcg(P.term_ctr) * npr;
     for (int q = threadIdx.x; q < npr; q += kThreads) {
       int i, j;
       pair_of(q, b, i, j);
       const int qb = pair_index(i, j, B);
       unsigned long long v = 0;
       for (int r = 0; r < P.replicas; ++r) v += __ldcg(P.gram_acc + (size_t)r * P.gram_stride + qb);
-      P.S_out[q] = mulmod(reduce(v, M), P.gram_mul, M);
+      S_out[q] = mulmod(reduce(v, M), P.gram_mul, M);
     }
     __syncthreads();
     for (int q = threadIdx.x; q < NP * P.replicas; q += kThreads)
       __stcg(P.gram_acc + (size_t)(q / NP) * P.gram_stride + q % NP, 0ull);
+    if (P.term_ctr != nullptr && threadIdx.x == 0) *P.term_ctr += 1u;  // read above by thread 0 only after the barrier
   }
   if (threadIdx.x == 0) atomicExch(P.counter, 0u);
 }
@@ -641,9 +645,19 @@ constexpr size_t pass_smem_bytes() {
   return (size_t)kWarps * 4 * (B >= 8 ? GramMma<B, 4>::kWords : GramCore<B, 4>::kWords);
 }
 
+// CTAs for a pass over `rows` rows: the resident maximum, but no more CTAs
+// than there are warp batches for (idle CTAs would still add their Gram
+// partials and lengthen the pass on small matrices).
+template <int B>
+static int pass_grid(const rr_krylov* kr, int64_t rows) {
+  const int64_t nbatch = (rows + Shape<B>::RPW - 1) / Shape<B>::RPW;
+  const int64_t need = (nbatch + kWarps - 1) / kWarps;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(kr->grid_pass, need));
+}
+
 template <int B>
 static int launch_pass_B(rr_krylov* kr, const PassParams& P, int mode) {
-  const dim3 grid(kr->grid_pass), block(kThreads);
+  const dim3 grid(pass_grid<B>(kr, P.rows)), block(kThreads);
   cudaStream_t s = kr->mat->ctx->stream;
   const size_t sm = pass_smem_bytes<B>();
   if (kr->fold4) {
@@ -681,7 +695,8 @@ static int launch_pass(rr_krylov* kr, const PassParams& P, int mode) {
 
 template <int B>
 static int launch_chunk_B(rr_krylov* kr, const ChunkParams& P) {
-  const dim3 grid(kr->grid_chunk), block(kThreads);
+  const dim3 grid((unsigned)std::max<int64_t>(1, std::min<int64_t>(kr->grid_chunk, (P.nchunks + kWarps - 1) / kWarps))),
+      block(kThreads);
   cudaStream_t s = kr->mat->ctx->stream;
   if (kr->fold4) chunk_kernel<B, 4><<<grid, block, 0, s>>>(P);
   else chunk_kernel<B, 2><<<grid, block, 0, s>>>(P);
@@ -837,7 +852,6 @@ static int run_chunks(rr_krylov* kr, const DevCsr& A, const uint32_t* X) {
 // ev (optional): four events recorded before pass 1, after pass 1, after the
 // chunks of pass 2 and after pass 2.
 int krylov_launch_application(rr_krylov* kr, cudaEvent_t* ev) {
-  const int np = kr->b * (kr->b + 1) / 2;
   rr_matrix* mat = kr->mat;
   cudaStream_t s = mat->ctx->stream;
   uint32_t* x = kr->X[kr->cur].ptr;
@@ -854,7 +868,9 @@ int krylov_launch_application(rr_krylov* kr, cudaEvent_t* ev) {
   P.Y = reinterpret_cast<uint4*>(kr->U.ptr);
   P.scale = kr->dr_m.ptr;
   P.gram_mul = kr->M.r1;  // the odd Gram is accumulated from z R^{-1}
-  P.S_out = kr->S.ptr + (size_t)(kr->len - kr->base) * np;
+  P.S_out = nullptr;  // slot len - base, from the device term counter
+  P.term_ctr = kr->d_term.ptr;
+  P.S_ptr = kr->d_sptr.ptr;
   RR_TRY(launch_pass(kr, P, kModeOdd));
   if (ev) RR_CUDA(cudaEventRecord(ev[1], s));
   // pass 2: rows of A^T
@@ -868,8 +884,7 @@ int krylov_launch_application(rr_krylov* kr, cudaEvent_t* ev) {
   P.Y = reinterpret_cast<uint4*>(xn);
   P.scale = kr->dc_m.ptr;
   P.scale2 = kr->dc_r.ptr;
-  P.gram_mul = 1;
-  P.S_out = kr->S.ptr + (size_t)(kr->len + 1 - kr->base) * np;
+  P.gram_mul = 1;  // slot len + 1 - base
   RR_TRY(launch_pass(kr, P, kModeEven));
   if (ev) RR_CUDA(cudaEventRecord(ev[3], s));
   kr->len += 2;

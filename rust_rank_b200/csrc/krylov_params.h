@@ -21,7 +21,12 @@ struct PassParams {
   int64_t gram_stride;            // words per replica (segments * B(B+1)/2)
   int replicas;                   // 1..kGramReplicas
   unsigned int* counter;
-  uint32_t* S_out;          // finished term, real pairs; nullptr = do not emit
+  uint32_t* S_out;          // finished term, real pairs; nullptr = do not emit (unless term_ctr)
+  // Device-indexed output (replayable launches, e.g. in a CUDA graph): the
+  // last CTA writes the term to (*S_ptr) + (*term_ctr) * pairs and advances
+  // *term_ctr.  nullptr = S_out as given.
+  unsigned int* term_ctr;
+  uint32_t* const* S_ptr;
   uint32_t gram_mul;        // factor applied to the finished term
   uint32_t w4, w5, w6;      // 2^32, 2^40, 2^48 mod p (limb weights of the tensor-core Gram)
   int b_real;

@@ -145,6 +145,16 @@ struct rr_krylov_s {
   int cur = 0;      // index of the current X
   int grid_pass = 0, grid_chunk = 0;
   int64_t launches = 0;  // kernels launched by this handle
+  // device-indexed sequence output: next slot (len - base) and the S pointer
+  rr::DevBuf<unsigned int> d_term;
+  rr::DevBuf<uint32_t*> d_sptr;
+  // a captured run of kGraphApps applications, replayable when cur == graph_cur
+  cudaGraphExec_t graph = nullptr;
+  int graph_cur = 0;
+  int64_t graph_launches = 0;
+  ~rr_krylov_s() {
+    if (graph) cudaGraphExecDestroy(graph);
+  }
 };
 
 namespace rr {
