@@ -246,6 +246,111 @@ def rank_pipeline(ctx, reps=3):
             "timing": "wall clock of rr_rank on a resident matrix, median of %d" % reps}
 
 
+def batched_vs_plain(ctx, nmat=48, rmin=1000, rmax=20000, b=16, workers=16):
+    """Graph-complex-like batch (rows log-uniform, cols = rows * U(0.6, 1), 3..10
+    entries +-1 per row, planted deficits): the batched engine (rr_batch_*)
+    against the plain one-matrix-at-a-time GPU loop (rr_rank) on the same set."""
+    import rust_rank_b200 as rr
+    from rust_rank_b200 import synth
+
+    mats = synth.graph_complex_batch(nmat=nmat, rmin=rmin, rmax=rmax)
+    drs, dcs, vs = [], [], []
+    for i, (_, _, _, m, n) in enumerate(mats):
+        dr, dc = synth.preconditioners(m, n, P, 100 + 10 * i)
+        drs.append(dr)
+        dcs.append(dc)
+        vs.append(synth.random_vectors(b, n, P, 101 + 10 * i))
+    t0 = time.perf_counter()
+    bt = rr.Batch(mats, b, P, drs, dcs, vs, ctx)
+    ranks = bt.ranks(workers)
+    t_batch = time.perf_counter() - t0
+    bt.close()
+    t0 = time.perf_counter()
+    plain = []
+    for i, (rowptr, col, val, m, n) in enumerate(mats):
+        dm = rr.CsrMatrix.from_arrays(rowptr, col, val, m, n).to_device(P, ctx)
+        plain.append(rr.block_wiedemann_rank(dm, b, P, row_precond=drs[i], col_precond=dcs[i], v=vs[i], ctx=ctx))
+        dm.close()
+    t_plain = time.perf_counter() - t0
+    assert list(ranks) == plain, "batched ranks differ from the plain loop"
+    return {"workload": f"graph_complex_batch_{nmat}_rows_{rmin}-{rmax}_b{b}",
+            "note": "rows scaled from 1000-200000 to keep the run within the bench's time budget",
+            "matrices": nmat, "batched_ranks_per_sec": nmat / t_batch, "plain_ranks_per_sec": nmat / t_plain,
+            "batched_over_plain": t_plain / t_batch, "batched_s": t_batch, "plain_s": t_plain,
+            "timing": "wall clock, host matrices in, ranks out (upload, Krylov, generator, readout)"}
+
+
+def served_stream(nreq=40, rmin=10_000, rmax=100_000, rate=50.0, b=16, seed=48):
+    """Poisson arrivals (mean `rate` req/s) of rank requests (rows log-uniform,
+    4..12 entries +-1 per row) through the rank service (rr_server_*), against
+    the plain sequential GPU loop on the same requests."""
+    import threading
+
+    import rust_rank_b200 as rr
+    from rust_rank_b200 import synth
+
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for i in range(nreq):
+        m = int(np.exp(rng.uniform(np.log(rmin), np.log(rmax))))
+        n = max(3, int(m * rng.uniform(0.6, 1.0)))
+        rowptr, col, val, m, n = synth.incidence_fast(m, n, 4, 12, n // 100 if i % 5 == 0 else 0, P, seed * 1000 + i)
+        dr, dc = synth.preconditioners(m, n, P, seed + 3 * i)
+        reqs.append((rowptr, col, val, m, n, dr, dc, synth.random_vectors(b, n, P, seed + 3 * i + 1)))
+    gaps = rng.exponential(1.0 / rate, size=nreq)
+    srv = rr.Server(b, P, lanes=4, workers=8, max_active=32, chunk_apps=64)
+    ids = [None] * nreq
+
+    def submitter():
+        t_next = time.perf_counter()
+        for i, r in enumerate(reqs):
+            t_next += gaps[i]
+            d = t_next - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            ids[i] = srv.submit(*r[:3], r[3], r[4], *r[5:])
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    th.join()
+    served = [srv.result(i, timeout=600.0)[0] for i in ids]
+    st = srv.stats()
+    srv.close()
+    ctx = rr.Context(0)
+    t0 = time.perf_counter()
+    plain = []
+    for r in reqs:
+        dm = rr.CsrMatrix.from_arrays(*r[:3], r[3], r[4]).to_device(P, ctx)
+        plain.append(rr.block_wiedemann_rank(dm, b, P, row_precond=r[5], col_precond=r[6], v=r[7], ctx=ctx))
+        dm.close()
+    t_plain = time.perf_counter() - t0
+    ctx.close()
+    assert served == plain, "served ranks differ from the plain loop"
+    return {"workload": f"served_poisson_{rate:g}rps_{nreq}req_rows_{rmin}-{rmax}_nnz4-12_b{b}",
+            "note": "rows scaled from 10^4-2*10^6 to keep the run within the bench's time budget",
+            "requests": nreq, "served_ranks_per_sec": st["ranks_per_s"], "p50_ms": st["p50_ms"],
+            "p99_ms": st["p99_ms"], "plain_ranks_per_sec": nreq / t_plain,
+            "served_over_plain": st["ranks_per_s"] / (nreq / t_plain),
+            "timing": "latency = submit to rank (queueing included); throughput = completions / (last completion - "
+                      "first submit); plain = sequential upload + rr_rank per request"}
+
+
+def pm_basis_stage(ctx, b=16, ds=(1 << 14, 1 << 16)):
+    """PM-basis alone on 2b x 2b generators of uniform random sequences."""
+    import rust_rank_b200 as rr
+
+    out = {}
+    rng = np.random.default_rng(4)
+    for d in ds:
+        seq = rng.integers(0, P, size=(b * (b + 1) // 2, d + 1), dtype=np.int64).astype(np.uint32)
+        t0 = time.perf_counter()
+        rr.PM_Basis(seq, d, P, ctx)
+        out[f"d{d}_ms"] = 1e3 * (time.perf_counter() - t0)
+    out["workload"] = f"pm_basis_b{b}_2b{2 * b}_uniform_random_seq"
+    out["timing"] = "wall clock of rr_pm_basis (host sequence in, generator out)"
+    return out
+
+
 def run_engine(args):
     import torch
 
@@ -341,6 +446,9 @@ def run_engine(args):
                                           "full matrix, oracle restatement of the reference CPU path"}
     if rank == 0 and world == 1 and not args.no_rank:
         line["rank_pipeline"] = rank_pipeline(ctx)
+        line["batched"] = batched_vs_plain(ctx)
+        line["served"] = served_stream()
+        line["pm_basis"] = pm_basis_stage(ctx)
     ks.close()
     dm.close()
     if rank == 0:

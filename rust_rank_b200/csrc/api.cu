@@ -334,16 +334,26 @@ constexpr int64_t kGraphApps = 16;
 constexpr int64_t kGraphMinRun = 2 * kGraphApps;
 
 // Captures kGraphApps applications (they are recorded, not run: the host
-// state the launches advance is restored afterwards).
+// state the launches advance is restored afterwards).  The capture runs on a
+// private stream, so other threads may keep queuing work on the context's
+// stream meanwhile; the graph is launched on the context's stream.
 static int capture_graph(rr_krylov* kr) {
-  cudaStream_t s = kr->mat->ctx->stream;
+  cudaStream_t s = nullptr;
+  RR_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
   const int64_t len0 = kr->len, launches0 = kr->launches;
   const int cur0 = kr->cur;
-  RR_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  const cudaError_t eb = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+  if (eb != cudaSuccess) {
+    cudaStreamDestroy(s);
+    RR_CUDA(eb);
+  }
+  kr->launch_stream = s;
   int st = RR_OK;
   for (int64_t i = 0; i < kGraphApps && st == RR_OK; ++i) st = krylov_launch_application(kr, nullptr);
   cudaGraph_t g = nullptr;
   const cudaError_t e = cudaStreamEndCapture(s, &g);
+  kr->launch_stream = nullptr;
+  cudaStreamDestroy(s);
   kr->graph_launches = kr->launches - launches0;
   kr->len = len0;
   kr->cur = cur0;

@@ -658,7 +658,7 @@ static int pass_grid(const rr_krylov* kr, int64_t rows) {
 template <int B>
 static int launch_pass_B(rr_krylov* kr, const PassParams& P, int mode) {
   const dim3 grid(pass_grid<B>(kr, P.rows)), block(kThreads);
-  cudaStream_t s = kr->mat->ctx->stream;
+  cudaStream_t s = kr->launch_stream ? kr->launch_stream : kr->mat->ctx->stream;
   const size_t sm = pass_smem_bytes<B>();
   if (kr->fold4) {
     if (mode == kModeInit) pass_kernel<B, kModeInit, 4><<<grid, block, sm, s>>>(P);
@@ -697,7 +697,7 @@ template <int B>
 static int launch_chunk_B(rr_krylov* kr, const ChunkParams& P) {
   const dim3 grid((unsigned)std::max<int64_t>(1, std::min<int64_t>(kr->grid_chunk, (P.nchunks + kWarps - 1) / kWarps))),
       block(kThreads);
-  cudaStream_t s = kr->mat->ctx->stream;
+  cudaStream_t s = kr->launch_stream ? kr->launch_stream : kr->mat->ctx->stream;
   if (kr->fold4) chunk_kernel<B, 4><<<grid, block, 0, s>>>(P);
   else chunk_kernel<B, 2><<<grid, block, 0, s>>>(P);
   RR_CUDA(cudaGetLastError());
@@ -853,7 +853,7 @@ static int run_chunks(rr_krylov* kr, const DevCsr& A, const uint32_t* X) {
 // chunks of pass 2 and after pass 2.
 int krylov_launch_application(rr_krylov* kr, cudaEvent_t* ev) {
   rr_matrix* mat = kr->mat;
-  cudaStream_t s = mat->ctx->stream;
+  cudaStream_t s = kr->launch_stream ? kr->launch_stream : mat->ctx->stream;
   uint32_t* x = kr->X[kr->cur].ptr;
   uint32_t* xn = kr->X[kr->cur ^ 1].ptr;
   if (ev) RR_CUDA(cudaEventRecord(ev[0], s));

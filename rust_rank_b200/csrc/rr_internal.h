@@ -150,6 +150,7 @@ struct rr_krylov_s {
   rr::DevBuf<uint32_t*> d_sptr;
   // a captured run of kGraphApps applications, replayable when cur == graph_cur
   cudaGraphExec_t graph = nullptr;
+  cudaStream_t launch_stream = nullptr;  // set while capturing (a private stream), else the context's
   int graph_cur = 0;
   int64_t graph_launches = 0;
   ~rr_krylov_s() {
