@@ -151,6 +151,13 @@ int rr_pm_basis_short_noalloc(const uint32_t* d_seq, int64_t seq_stride, int32_t
 int rr_rank_from_basis(const uint32_t* M, const int64_t* delta, int32_t b, int64_t len, uint32_t p,
                        int64_t* rank);
 
+/* rr_pm_basis for `count` sequences with the same b, d and p, solved in
+ * lockstep on the device (one launch per step of the recursion for all of
+ * them); seqs[z] is [b(b+1)/2][seq_strides[z] >= nlen], M[z] and delta[z] as
+ * for rr_pm_basis.  Each result equals rr_pm_basis on that sequence alone. */
+int rr_pm_basis_batch(rr_ctx* ctx, int32_t count, const uint32_t* const* seqs, const int64_t* seq_strides, int32_t b,
+                      int64_t nlen, int64_t d, uint32_t p, uint32_t* const* M, int64_t* const* delta);
+
 /* Whole pipeline (src/main.rs:463-606): sequence length rule of
  * src/main.rs:497-504 when max_nlen == 0, Krylov sequence, PM-basis with
  * d = largest power of two <= length, rank readout. */

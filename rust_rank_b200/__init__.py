@@ -293,6 +293,27 @@ def PM_Basis(seq: np.ndarray, d: int, seqprime: int, ctx: Context | None = None)
     return M, delta
 
 
+def PM_Basis_batch(seqs, d: int, seqprime: int, ctx: Context | None = None):
+    """PM_Basis of several sequences of equal shape solved in lockstep
+    (rr_pm_basis_batch); returns [(M, delta)] in order."""
+    ctx = ctx or default_context()
+    seqs = [np.ascontiguousarray(s, np.uint32) for s in seqs]
+    nn, nlen = seqs[0].shape
+    b = int((np.sqrt(8 * nn + 1) - 1) // 2)
+    if b * (b + 1) // 2 != nn or any(s.shape != seqs[0].shape for s in seqs):
+        raise ValueError("sequences must share one square block size and length")
+    dd = 1
+    while dd < d:
+        dd *= 2
+    Ms = [np.zeros((2 * b, 2 * b, dd + 1), np.uint32) for _ in seqs]
+    ds = [np.zeros(2 * b, np.int64) for _ in seqs]
+    cnt = len(seqs)
+    arr = lambda xs: (C.c_void_p * cnt)(*[x.ctypes.data for x in xs])  # noqa: E731
+    strides = np.full(cnt, nlen, np.int64)
+    check(lib().rr_pm_basis_batch(ctx.handle, cnt, arr(seqs), ptr(strides), b, nlen, dd, seqprime, arr(Ms), arr(ds)))
+    return list(zip(Ms, ds))
+
+
 def analyze_pm_basis(basis: np.ndarray, delta: np.ndarray, p: int) -> int:
     """src/sigma_basis.rs:71-152 -> src/blockbmtest.rs:574-599; returns the estimated rank."""
     basis = np.ascontiguousarray(basis, np.uint32)

@@ -513,6 +513,22 @@ int rr_pm_basis(rr_ctx* ctx, const uint32_t* seq, int64_t seq_stride, int32_t b,
   return pm_basis_device(ctx, seq, seq_stride, b, nlen, dd, p, M, delta);
 }
 
+int rr_pm_basis_batch(rr_ctx* ctx, int32_t count, const uint32_t* const* seqs, const int64_t* seq_strides, int32_t b,
+                      int64_t nlen, int64_t d, uint32_t p, uint32_t* const* M, int64_t* const* delta) {
+  if (!ctx || count < 0 || (count > 0 && (!seqs || !seq_strides || !M || !delta))) return fail(RR_EINVAL, "NULL argument");
+  RR_TRY(rr_prime_check(p));
+  if (b < 1 || b > 32) return fail(RR_EINVAL, "b = %d must be in [1, 32]", b);
+  int64_t dd = 1;
+  while (dd < d) dd *= 2;
+  if (dd >= nlen) return fail(RR_EINVAL, "sequence too short: d = %lld, nlen = %lld", (long long)dd, (long long)nlen);
+  for (int z = 0; z < count; ++z) {
+    if (!seqs[z] || !M[z] || !delta[z]) return fail(RR_EINVAL, "NULL array for generator %d", z);
+    if (seq_strides[z] < nlen) return fail(RR_EINVAL, "seq_strides[%d] < nlen", z);
+  }
+  RR_CUDA(cudaSetDevice(ctx->device));
+  return pm_basis_batch_device(ctx, count, seqs, seq_strides, b, dd, p, M, delta);
+}
+
 int rr_rank_from_basis(const uint32_t* M, const int64_t* delta, int32_t b, int64_t len, uint32_t p, int64_t* rank) {
   if (!M || !delta || !rank) return fail(RR_EINVAL, "NULL argument");
   if (b < 1 || len < 1) return fail(RR_EINVAL, "bad sizes");

@@ -9,10 +9,11 @@
 // application t form a suffix of the stack and the passes start at that
 // suffix.  Each application of B is then two launches for the whole batch.
 //
-// The generators are independent: rr_batch_ranks runs them on several streams
-// at once (one host thread and one context per stream, stream-ordered
-// allocations), so that the one-CTA leaf kernels of different matrices occupy
-// different SMs.
+// The generators: matrices with equal sequence length finish their Krylov
+// loops together and are solved in lockstep by one batched PM-basis (one
+// leaf-kernel CTA per matrix, one launch per product step for all of them);
+// rr_batch_ranks runs these jobs on a few streams at once (one host thread
+// and one context per stream), as soon as their sequences are complete.
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -436,7 +437,6 @@ int rr_batch_ranks(rr_batch* bt, int32_t workers, int64_t* ranks) {
   if (!bt || !ranks) return fail(RR_EINVAL, "NULL argument");
   RR_CUDA(cudaSetDevice(bt->ctx->device));
   const int nmat = bt->nmat, np = bt->np, b = bt->b;
-  workers = std::max(1, std::min(workers, nmat));
   std::vector<cudaEvent_t> ev(nmat, nullptr);
   Progress prog;
   const bool overlap = !bt->done;
@@ -451,6 +451,26 @@ int rr_batch_ranks(rr_batch* bt, int32_t workers, int64_t* ranks) {
   } else {
     prog.published = nmat;
   }
+  // generator jobs: runs of stack positions with equal sequence length (they
+  // finish their Krylov loops together), solved in lockstep by one batched
+  // PM-basis each, split so that a job's workspace stays within a budget
+  struct Job { int first, count; };
+  std::vector<Job> jobs;
+  {
+    constexpr size_t kJobBudget = (size_t)8 << 30;
+    for (int s0 = 0; s0 < nmat;) {
+      int s1 = s0;
+      while (s1 < nmat && bt->apps[s1] == bt->apps[s0]) ++s1;
+      const int64_t L = 2 * bt->apps[s0] + 1;
+      int64_t d = 1;
+      while (d <= L) d *= 2;
+      d /= 2;
+      const int per = (int)std::max<size_t>(1, kJobBudget / pm_workspace_bytes(b, d));
+      for (int q = s0; q < s1; q += per) jobs.push_back({q, std::min(per, s1 - q)});
+      s0 = s1;
+    }
+  }
+  workers = std::max(1, std::min(workers, (int)jobs.size()));
   std::atomic<int> next{0};
   std::vector<int> status(workers, RR_OK);
   std::vector<std::string> errors(workers);
@@ -459,37 +479,51 @@ int rr_batch_ranks(rr_batch* bt, int32_t workers, int64_t* ranks) {
     rr_ctx* c = nullptr;
     int rc = rr_ctx_create(bt->ctx->device, &c);
     if (rc != RR_OK) { status[w] = rc; errors[w] = rr_last_error(); return; }
-    std::vector<uint32_t> raw, seq, Mv;
+    std::vector<uint32_t> raw;
     for (;;) {
-      const int s = next.fetch_add(1);
-      if (s >= nmat) break;
+      const int j = next.fetch_add(1);
+      if (j >= (int)jobs.size()) break;
+      const int first = jobs[j].first, cnt = jobs[j].count, last = first + cnt - 1;
       {
         std::unique_lock<std::mutex> lk(prog.mu);
-        prog.cv.wait(lk, [&] { return prog.published > s || prog.failed; });
-        if (prog.published <= s) break;  // the Krylov loop failed
+        prog.cv.wait(lk, [&] { return prog.published > last || prog.failed; });
+        if (prog.published <= last) break;  // the Krylov loop failed
       }
-      const int64_t L = 2 * bt->apps[s] + 1;
-      raw.resize((size_t)np * L);
+      const int64_t L = 2 * bt->apps[first] + 1;
+      int64_t d = 1;  // src/main.rs:599-603
+      while (d <= L) d *= 2;
+      d /= 2;
+      std::vector<std::vector<uint32_t>> seq(cnt), Mv(cnt);
+      std::vector<std::vector<int64_t>> delta(cnt);
+      std::vector<const uint32_t*> sp(cnt);
+      std::vector<uint32_t*> mp(cnt);
+      std::vector<int64_t*> dp(cnt);
+      std::vector<int64_t> strides(cnt, L);
       cudaError_t e = cudaSuccess;
-      if (overlap) e = cudaStreamWaitEvent(c->stream, ev[s], 0);
-      if (e == cudaSuccess)
+      if (overlap) e = cudaStreamWaitEvent(c->stream, ev[last], 0);
+      raw.resize((size_t)np * L);
+      for (int z = 0; z < cnt && e == cudaSuccess; ++z) {
+        const int s = first + z;
         e = cudaMemcpyAsync(raw.data(), bt->S.ptr + bt->s_off[s], raw.size() * 4, cudaMemcpyDeviceToHost, c->stream);
-      if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) break;
+        seq[z].resize(raw.size());
+        for (int64_t t = 0; t < L; ++t)
+          for (int q = 0; q < np; ++q) seq[z][(size_t)q * L + t] = raw[(size_t)t * np + q];
+        Mv[z].resize((size_t)(2 * b) * (2 * b) * (d + 1));
+        delta[z].resize(2 * b);
+        sp[z] = seq[z].data();
+        mp[z] = Mv[z].data();
+        dp[z] = delta[z].data();
+      }
       if (e != cudaSuccess) {
         status[w] = RR_ECUDA;
         errors[w] = cudaGetErrorString(e);
         break;
       }
-      seq.resize(raw.size());
-      for (int64_t t = 0; t < L; ++t)
-        for (int q = 0; q < np; ++q) seq[(size_t)q * L + t] = raw[(size_t)t * np + q];
-      int64_t d = 1;  // src/main.rs:599-603
-      while (d <= L) d *= 2;
-      d /= 2;
-      Mv.resize((size_t)(2 * b) * (2 * b) * (d + 1));
-      std::vector<int64_t> delta(2 * b);
-      rc = rr_pm_basis(c, seq.data(), L, b, L, d, bt->p, Mv.data(), delta.data());
-      if (rc == RR_OK) rc = rr_rank_from_basis(Mv.data(), delta.data(), b, d + 1, bt->p, &ranks[bt->order[s]]);
+      rc = pm_basis_batch_device(c, cnt, sp.data(), strides.data(), b, d, bt->p, mp.data(), dp.data());
+      for (int z = 0; z < cnt && rc == RR_OK; ++z)
+        rc = rr_rank_from_basis(Mv[z].data(), delta[z].data(), b, d + 1, bt->p, &ranks[bt->order[first + z]]);
       if (rc != RR_OK) { status[w] = rc; errors[w] = rr_last_error(); break; }
     }
     rr_ctx_destroy(c);

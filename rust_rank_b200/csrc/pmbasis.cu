@@ -58,17 +58,30 @@ __device__ __forceinline__ uint32_t mul_shoup(uint32_t a, uint32_t w, uint32_t w
   return r >= p ? r - p : r;
 }
 
+// A batch of strided polynomial matrices seen as a flat list of polynomials:
+// polynomial q is entry (qi / cols, qi % cols) of matrix q / npb (qi = q % npb),
+// starting at p + (q / npb) * bs + (qi / cols) * rs + (qi % cols) * cs.
+struct PolyView {
+  uint32_t* p;
+  int cols, npb;
+  int64_t rs, cs, bs;
+  __host__ __device__ uint32_t* at(int64_t q) const {
+    const int64_t bi = q / npb, qi = q % npb;
+    return p + bi * bs + (qi / cols) * rs + (qi % cols) * cs;
+  }
+};
+
 // ---------------------------------------------------------------- NTT kernels
 // Forward DIF stage with butterfly span `len` (len > kNttBlock) in global memory.
 __global__ void ntt_fwd_stage_kernel(uint32_t* a, int64_t N, int64_t npoly, int64_t len, Twiddles tw, uint32_t p) {
   const int64_t half = len / 2;
-  const int64_t per = N / 2;
-  const int64_t total = npoly * per;
+  const int lh = __ffsll(half) - 1, lp = __ffsll(N / 2) - 1;
+  const int64_t total = npoly * (N / 2);
   const int64_t tstep = tw.nmax / len;
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t poly = t / per, b = t % per;
-    const int64_t j = b % half;
-    uint32_t* x = a + poly * N + (b / half) * len + j;
+    const int64_t poly = t >> lp, b = t & (N / 2 - 1);
+    const int64_t j = b & (half - 1);
+    uint32_t* x = a + poly * N + ((b >> lh) << (lh + 1)) + j;
     const uint32_t u = x[0], v = x[half];
     x[0] = addmod(u, v, p);
     x[half] = mul_shoup(submod(u, v, p), tw.w[j * tstep], tw.ws[j * tstep], p);
@@ -78,13 +91,13 @@ __global__ void ntt_fwd_stage_kernel(uint32_t* a, int64_t N, int64_t npoly, int6
 // Inverse DIT stage with span len (len > kNttBlock) in global memory.
 __global__ void ntt_inv_stage_kernel(uint32_t* a, int64_t N, int64_t npoly, int64_t len, Twiddles tw, uint32_t p) {
   const int64_t half = len / 2;
-  const int64_t per = N / 2;
-  const int64_t total = npoly * per;
+  const int lh = __ffsll(half) - 1, lp = __ffsll(N / 2) - 1;
+  const int64_t total = npoly * (N / 2);
   const int64_t tstep = tw.nmax / len;
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t poly = t / per, b = t % per;
-    const int64_t j = b % half;
-    uint32_t* x = a + poly * N + (b / half) * len + j;
+    const int64_t poly = t >> lp, b = t & (N / 2 - 1);
+    const int64_t j = b & (half - 1);
+    uint32_t* x = a + poly * N + ((b >> lh) << (lh + 1)) + j;
     const uint32_t u = x[0];
     const uint32_t v = mul_shoup(x[half], tw.w[j * tstep], tw.ws[j * tstep], p);
     x[0] = addmod(u, v, p);
@@ -92,104 +105,191 @@ __global__ void ntt_inv_stage_kernel(uint32_t* a, int64_t N, int64_t npoly, int6
   }
 }
 
-// Forward transform of the last stages (span <= T = min(N, kNttBlock)) of each
-// block of T elements in shared memory.  When src != nullptr the block is
-// first loaded from src (poly q: src[(q / src_cols) * src_rs + (q % src_cols) * src_cs + t],
-// t < src_len, zero padded) -- only valid when N <= kNttBlock.
-__global__ void __launch_bounds__(512) ntt_fwd_smem_kernel(uint32_t* a, int64_t N, int T, const uint32_t* src,
-                                                           int src_cols, int64_t src_rs, int64_t src_cs,
-                                                           int64_t src_len, Twiddles tw, uint32_t p) {
-  __shared__ uint32_t s[kNttBlock];
-  const int64_t blocks_per_poly = N / T;
-  const int64_t poly = blockIdx.x / blocks_per_poly;
-  const int64_t off = (blockIdx.x % blocks_per_poly) * T;
-  uint32_t* x = a + poly * N + off;
-  if (src) {
-    const uint32_t* sp = src + (poly / src_cols) * src_rs + (poly % src_cols) * src_cs;
-    for (int t = threadIdx.x; t < T; t += blockDim.x) s[t] = (t < src_len) ? sp[t] : 0u;
-  } else {
-    for (int t = threadIdx.x; t < T; t += blockDim.x) s[t] = x[t];
+// Shared-memory NTT of the last (forward) or first (inverse) stages, span up
+// to T = 2^logT <= kNttBlock.  A CTA transforms G = max(1, kNttGroup / T)
+// consecutive T-blocks (several short polynomials per CTA), with the twiddles
+// of span T staged in shared memory (span 2^lg uses entry j << (logT - lg))
+// and power-of-two index arithmetic.  Dynamic shared memory: (G + 1) * T words.
+constexpr int kNttGroup = 2048;
+
+__device__ __forceinline__ void ntt_load_twiddles(uint32_t* W, uint32_t* WS, int logT, const Twiddles& tw) {
+  const int64_t tstep = tw.nmax >> logT;
+  for (int j = threadIdx.x; j < (1 << (logT - 1)); j += blockDim.x) {
+    W[j] = tw.w[j * tstep];
+    WS[j] = tw.ws[j * tstep];
+  }
+}
+
+// Forward DIF.  When src.p != nullptr the blocks are first loaded from the
+// polynomials of src (t < src_len, zero padded) -- only valid when N <= kNttBlock.
+__global__ void __launch_bounds__(512) ntt_fwd_smem_kernel(uint32_t* a, int64_t N, int logT, int64_t nblocks,
+                                                           PolyView src, int64_t src_len, Twiddles tw, uint32_t p) {
+  extern __shared__ uint32_t nsm[];
+  const int T = 1 << logT, G = T >= kNttGroup ? 1 : kNttGroup / T;
+  uint32_t* s = nsm;
+  uint32_t* W = s + G * T;
+  uint32_t* WS = W + T / 2;
+  const int64_t blk0 = (int64_t)blockIdx.x * G;
+  ntt_load_twiddles(W, WS, logT, tw);
+  for (int e = threadIdx.x; e < G * T; e += blockDim.x) {
+    const int g = e >> logT, t = e & (T - 1);
+    const int64_t blk = blk0 + g;
+    uint32_t v = 0;
+    if (blk < nblocks) {
+      if (src.p) v = t < src_len ? src.at(blk)[t] : 0u;  // N == T: block = polynomial
+      else v = a[(blk << logT) + t];
+    }
+    s[e] = v;
   }
   __syncthreads();
-  for (int len = T; len >= 2; len >>= 1) {
-    const int half = len / 2;
-    const int64_t tstep = tw.nmax / len;
-    for (int b = threadIdx.x; b < T / 2; b += blockDim.x) {
-      const int j = b % half;
-      const int i0 = (b / half) * len + j;
+  const int nbf = G * T / 2;
+  for (int lg = logT; lg >= 1; --lg) {
+    const int lh = lg - 1, half = 1 << lh, sh = logT - lg;
+    for (int bf = threadIdx.x; bf < nbf; bf += blockDim.x) {
+      const int j = bf & (half - 1);
+      const int i0 = ((bf >> lh) << lg) | j;
       const uint32_t u = s[i0], v = s[i0 + half];
       s[i0] = addmod(u, v, p);
-      s[i0 + half] = mul_shoup(submod(u, v, p), tw.w[j * tstep], tw.ws[j * tstep], p);
+      s[i0 + half] = mul_shoup(submod(u, v, p), W[j << sh], WS[j << sh], p);
     }
     __syncthreads();
   }
-  for (int t = threadIdx.x; t < T; t += blockDim.x) x[t] = s[t];
+  for (int e = threadIdx.x; e < G * T; e += blockDim.x) {
+    const int64_t blk = blk0 + (e >> logT);
+    if (blk < nblocks) a[(blk << logT) + (e & (T - 1))] = s[e];
+  }
 }
 
-// Inverse transform of the first stages (span <= T) in shared memory.  When
-// dst != nullptr (only valid when N <= T) the result is scaled by N^{-1} and
-// coefficients [lo, lo + cnt) are written to dst[(q / dst_cols) * dst_rs + (q % dst_cols) * dst_cs + t].
-__global__ void __launch_bounds__(512) ntt_inv_smem_kernel(uint32_t* a, int64_t N, int T, uint32_t* dst, int dst_cols,
-                                                           int64_t dst_rs, int64_t dst_cs, int64_t lo, int64_t cnt,
-                                                           uint32_t ninv, uint32_t ninv_s, Twiddles tw, uint32_t p) {
-  __shared__ uint32_t s[kNttBlock];
-  const int64_t blocks_per_poly = N / T;
-  const int64_t poly = blockIdx.x / blocks_per_poly;
-  const int64_t off = (blockIdx.x % blocks_per_poly) * T;
-  uint32_t* x = a + poly * N + off;
-  for (int t = threadIdx.x; t < T; t += blockDim.x) s[t] = x[t];
+// Inverse DIT of the first stages.  When dst.p != nullptr (only valid when
+// N <= T) the result is scaled by N^{-1} and coefficients [lo, lo + cnt) go to
+// the polynomials of dst.
+__global__ void __launch_bounds__(512) ntt_inv_smem_kernel(uint32_t* a, int64_t N, int logT, int64_t nblocks,
+                                                           PolyView dst, int64_t lo, int64_t cnt, uint32_t ninv,
+                                                           uint32_t ninv_s, Twiddles tw, uint32_t p) {
+  extern __shared__ uint32_t nsm[];
+  const int T = 1 << logT, G = T >= kNttGroup ? 1 : kNttGroup / T;
+  uint32_t* s = nsm;
+  uint32_t* W = s + G * T;
+  uint32_t* WS = W + T / 2;
+  const int64_t blk0 = (int64_t)blockIdx.x * G;
+  ntt_load_twiddles(W, WS, logT, tw);
+  for (int e = threadIdx.x; e < G * T; e += blockDim.x) {
+    const int64_t blk = blk0 + (e >> logT);
+    s[e] = blk < nblocks ? a[(blk << logT) + (e & (T - 1))] : 0u;
+  }
   __syncthreads();
-  for (int len = 2; len <= T; len <<= 1) {
-    const int half = len / 2;
-    const int64_t tstep = tw.nmax / len;
-    for (int b = threadIdx.x; b < T / 2; b += blockDim.x) {
-      const int j = b % half;
-      const int i0 = (b / half) * len + j;
+  const int nbf = G * T / 2;
+  for (int lg = 1; lg <= logT; ++lg) {
+    const int lh = lg - 1, half = 1 << lh, sh = logT - lg;
+    for (int bf = threadIdx.x; bf < nbf; bf += blockDim.x) {
+      const int j = bf & (half - 1);
+      const int i0 = ((bf >> lh) << lg) | j;
       const uint32_t u = s[i0];
-      const uint32_t v = mul_shoup(s[i0 + half], tw.w[j * tstep], tw.ws[j * tstep], p);
+      const uint32_t v = mul_shoup(s[i0 + half], W[j << sh], WS[j << sh], p);
       s[i0] = addmod(u, v, p);
       s[i0 + half] = submod(u, v, p);
     }
     __syncthreads();
   }
-  if (dst) {
-    uint32_t* dp = dst + (poly / dst_cols) * dst_rs + (poly % dst_cols) * dst_cs;
-    for (int64_t t = threadIdx.x; t < cnt; t += blockDim.x) dp[t] = mul_shoup(s[lo + t], ninv, ninv_s, p);
+  if (dst.p) {
+    for (int e = threadIdx.x; e < G * cnt; e += blockDim.x) {
+      const int g = (int)(e / cnt);
+      const int64_t t = e - (int64_t)g * cnt;
+      const int64_t blk = blk0 + g;
+      if (blk < nblocks) dst.at(blk)[t] = mul_shoup(s[(g << logT) + lo + t], ninv, ninv_s, p);
+    }
   } else {
-    for (int t = threadIdx.x; t < T; t += blockDim.x) x[t] = s[t];
+    for (int e = threadIdx.x; e < G * T; e += blockDim.x) {
+      const int64_t blk = blk0 + (e >> logT);
+      if (blk < nblocks) a[(blk << logT) + (e & (T - 1))] = s[e];
+    }
   }
 }
 
 // Copy poly q of a strided source into a dense N-length slot with zero padding.
-__global__ void pad_copy_kernel(uint32_t* a, int64_t N, int64_t npoly, const uint32_t* src, int src_cols, int64_t src_rs,
-                                int64_t src_cs, int64_t src_len) {
+__global__ void pad_copy_kernel(uint32_t* a, int64_t N, int64_t npoly, PolyView src, int64_t src_len) {
   const int64_t total = npoly * N;
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
     const int64_t q = t / N, k = t % N;
-    a[t] = (k < src_len) ? src[(q / src_cols) * src_rs + (q % src_cols) * src_cs + k] : 0u;
+    a[t] = (k < src_len) ? src.at(q)[k] : 0u;
   }
 }
 
-__global__ void extract_scale_kernel(const uint32_t* a, int64_t N, int64_t npoly, uint32_t* dst, int dst_cols,
-                                     int64_t dst_rs, int64_t dst_cs, int64_t lo, int64_t cnt, uint32_t ninv,
-                                     uint32_t ninv_s, uint32_t p) {
+__global__ void extract_scale_kernel(const uint32_t* a, int64_t N, int64_t npoly, PolyView dst, int64_t lo, int64_t cnt,
+                                     uint32_t ninv, uint32_t ninv_s, uint32_t p) {
   const int64_t total = npoly * cnt;
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
     const int64_t q = t / cnt, k = t % cnt;
-    dst[(q / dst_cols) * dst_rs + (q % dst_cols) * dst_cs + k] = mul_shoup(a[q * N + lo + k], ninv, ninv_s, p);
+    dst.at(q)[k] = mul_shoup(a[q * N + lo + k], ninv, ninv_s, p);
   }
 }
 
-// Pointwise stage: C[i][j][f] = sum_r A[i][r][f] * B[r][j][f]  (all N-length).
-__global__ void pointwise_kernel(const uint32_t* __restrict__ A, const uint32_t* __restrict__ Bm, uint32_t* __restrict__ C,
-                                 int m, int r, int k, int64_t N, ModP M) {
-  const int64_t total = (int64_t)m * k * N;
+// Pointwise stage: C[i][j][f] = sum_r A[i][r][f] * B[r][j][f]  (all N-length),
+// for nb matrices stored one after the other.  A thread computes a 4 x 4 tile
+// of (i, j) at one frequency (consecutive threads take consecutive
+// frequencies, so every load is coalesced), 16 carry-chain accumulators,
+// folded every 4 steps (every 2 for primes where 4 products do not fit).  m and k are multiples of 4 here (m = 2b, k in {b, 2b}
+// with b a multiple of 4); pointwise1_kernel covers the rest.
+__global__ void __launch_bounds__(256) pointwise_kernel(const uint32_t* __restrict__ A, const uint32_t* __restrict__ Bm,
+                                                        uint32_t* __restrict__ C, int m, int r, int k, int64_t N, int nb,
+                                                        int fold_mask, ModP M) {
+  const int ti = m / 4, tj = k / 4;
+  const int64_t per = (int64_t)ti * tj * N;
+  const int64_t total = per * nb;
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t f = t % N;
-    const int64_t ij = t / N;
+    const int64_t bi = t / per, tt = t - bi * per;
+    const int64_t f = tt % N;
+    const int64_t tile = tt / N;
+    const int i0 = 4 * (int)(tile / tj), j0 = 4 * (int)(tile % tj);
+    const uint32_t* a = A + bi * (int64_t)m * r * N + (int64_t)i0 * r * N + f;
+    const uint32_t* b = Bm + bi * (int64_t)r * k * N + (int64_t)j0 * N + f;
+    uint32_t lo[4][4], hi[4][4];
+#pragma unroll
+    for (int x = 0; x < 4; ++x)
+#pragma unroll
+      for (int y = 0; y < 4; ++y) lo[x][y] = hi[x][y] = 0;
+    for (int s = 0; s < r; ++s) {
+      uint32_t av[4], bv[4];
+#pragma unroll
+      for (int x = 0; x < 4; ++x) av[x] = a[(int64_t)x * r * N + (int64_t)s * N];
+#pragma unroll
+      for (int y = 0; y < 4; ++y) bv[y] = b[(int64_t)s * k * N + (int64_t)y * N];
+#pragma unroll
+      for (int x = 0; x < 4; ++x)
+#pragma unroll
+        for (int y = 0; y < 4; ++y) mac_cc(av[x], bv[y], lo[x][y], hi[x][y]);
+      if ((s & fold_mask) == fold_mask) {  // fold (hi:lo) -> hi * (2^32 mod p) + lo every 4 (or 2) products
+#pragma unroll
+        for (int x = 0; x < 4; ++x)
+#pragma unroll
+          for (int y = 0; y < 4; ++y) {
+            const uint32_t h = hi[x][y];
+            hi[x][y] = 0;
+            mac_cc(h, M.c32, lo[x][y], hi[x][y]);
+          }
+      }
+    }
+    uint32_t* c = C + bi * (int64_t)m * k * N + (int64_t)i0 * k * N + (int64_t)j0 * N + f;
+#pragma unroll
+    for (int x = 0; x < 4; ++x)
+#pragma unroll
+      for (int y = 0; y < 4; ++y)
+        c[(int64_t)x * k * N + (int64_t)y * N] = reduce(((uint64_t)hi[x][y] << 32) | lo[x][y], M);
+  }
+}
+
+// Pointwise stage for shapes that are not multiples of 4 (one output per thread).
+__global__ void pointwise1_kernel(const uint32_t* __restrict__ A, const uint32_t* __restrict__ Bm, uint32_t* __restrict__ C,
+                                  int m, int r, int k, int64_t N, int nb, ModP M) {
+  const int64_t per = (int64_t)m * k * N;
+  const int64_t total = per * nb;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t bi = t / per, tt = t % per;
+    const int64_t f = tt % N;
+    const int64_t ij = tt / N;
     const int i = (int)(ij / k), j = (int)(ij % k);
-    const uint32_t* a = A + (int64_t)i * r * N + f;
-    const uint32_t* b = Bm + (int64_t)j * N + f;
+    const uint32_t* a = A + bi * (int64_t)m * r * N + (int64_t)i * r * N + f;
+    const uint32_t* b = Bm + bi * (int64_t)r * k * N + (int64_t)j * N + f;
     uint64_t acc = 0;
     int s = 0;
     for (; s + 1 < r; s += 2) {
@@ -205,18 +305,21 @@ __global__ void pointwise_kernel(const uint32_t* __restrict__ A, const uint32_t*
 // Direct product for moduli without a suitable NTT: dst coefficient lo + t of
 // sum_s A[i][s] * B[s][j], one thread per output coefficient.
 __global__ void schoolbook_kernel(const uint32_t* A, int mA, int r, int64_t la, int64_t a_rs, int64_t a_cs,
-                                  const uint32_t* Bm, int k, int64_t lb, int64_t b_rs, int64_t b_cs, uint32_t* dst,
-                                  int64_t d_rs, int64_t d_cs, int64_t lo, int64_t cnt, ModP M) {
-  const int64_t total = (int64_t)mA * k * cnt;
+                                  int64_t a_bs, const uint32_t* Bm, int k, int64_t lb, int64_t b_rs, int64_t b_cs,
+                                  int64_t b_bs, uint32_t* dst, int64_t d_rs, int64_t d_cs, int64_t d_bs, int64_t lo,
+                                  int64_t cnt, int nb, ModP M) {
+  const int64_t per = (int64_t)mA * k * cnt;
+  const int64_t total = per * nb;
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t c = lo + t % cnt;
-    const int64_t ij = t / cnt;
+    const int64_t bi = t / per, tt = t % per;
+    const int64_t c = lo + tt % cnt;
+    const int64_t ij = tt / cnt;
     const int i = (int)(ij / k), j = (int)(ij % k);
     uint64_t acc = 0;
     int parity = 0;
     for (int s = 0; s < r; ++s) {
-      const uint32_t* a = A + (int64_t)i * a_rs + (int64_t)s * a_cs;
-      const uint32_t* b = Bm + (int64_t)s * b_rs + (int64_t)j * b_cs;
+      const uint32_t* a = A + bi * a_bs + (int64_t)i * a_rs + (int64_t)s * a_cs;
+      const uint32_t* b = Bm + bi * b_bs + (int64_t)s * b_rs + (int64_t)j * b_cs;
       const int64_t u0 = c - (lb - 1) > 0 ? c - (lb - 1) : 0;
       const int64_t u1 = c < la - 1 ? c : la - 1;
       for (int64_t u = u0; u <= u1; ++u) {
@@ -224,7 +327,7 @@ __global__ void schoolbook_kernel(const uint32_t* A, int mA, int r, int64_t la, 
         if (++parity == 2) { acc = fold(acc, M); parity = 0; }
       }
     }
-    dst[(int64_t)i * d_rs + (int64_t)j * d_cs + (c - lo)] = reduce(acc, M);
+    dst[bi * d_bs + (int64_t)i * d_rs + (int64_t)j * d_cs + (c - lo)] = reduce(acc, M);
   }
 }
 
@@ -519,14 +622,14 @@ constexpr int kLeafWarps = kLeafThreads / 32;
 
 
 struct LeafParams {
-  const uint32_t* G;  // G[i][c][t] (row stride g_rs, column stride g_cs), t < K
-  int64_t g_rs, g_cs;
+  const uint32_t* G;  // G[i][c][t] (row stride g_rs, column stride g_cs), t < K; CTA z takes G + z g_bs
+  int64_t g_rs, g_cs, g_bs;
   int m, n, K;
   int64_t cs;                // words per residual coefficient in shared memory (>= m * n, padded)
-  int64_t* delta;            // [m], in/out
-  uint32_t* Tt;              // [K][m][m]: Tt[k][s][i] = stored T_k[i][s]
-  unsigned long long* mask;  // [K]: bit i set when row i of leaf k is a pivot row (an "x" row)
-  uint32_t* sigma_inv;       // [m]: inverse row scales of the block's stored basis
+  int64_t* delta;            // [nb][m], in/out
+  uint32_t* Tt;              // [nb][K][m][m]: Tt[k][s][i] = stored T_k[i][s]
+  unsigned long long* mask;  // [nb][K]: bit i set when row i of leaf k is a pivot row (an "x" row)
+  uint32_t* sigma_inv;       // [nb][m]: inverse row scales of the block's stored basis
   ModP M;
   int* status;
 };
@@ -592,8 +695,19 @@ __device__ __forceinline__ int leaf_slot(unsigned long long mx, int i, int m) {
   return ((nx + 3) & ~3) + __popcll(~mx & valid & below);
 }
 
+// One matrix of the batch per CTA (blockIdx.x).
+__device__ __forceinline__ void leaf_select(LeafParams& P) {
+  const int z = blockIdx.x;
+  P.G += (int64_t)z * P.g_bs;
+  P.delta += (int64_t)z * P.m;
+  P.Tt += (int64_t)z * P.K * P.m * P.m;
+  P.mask += (int64_t)z * P.K;
+  P.sigma_inv += (int64_t)z * P.m;
+}
+
 template <int CT, int FE>
 __global__ void __launch_bounds__(kLeafThreads) pm_leaves_kernel(LeafParams P) {
+  leaf_select(P);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int m = P.m, n = P.n, K = P.K;
   const int W = n + m;
@@ -848,6 +962,7 @@ __device__ __forceinline__ void plane_store(uint32_t* coeff, int NPc, int col, i
 }
 
 __global__ void __launch_bounds__(kLeafThreads) pm_leaves_mma_kernel(LeafParams P) {
+  leaf_select(P);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int m = P.m, n = P.n, K = P.K;
   const int W = n + m;
@@ -1084,8 +1199,14 @@ template <int FE>
 __global__ void __launch_bounds__(256) pm_block_basis_kernel(const uint32_t* __restrict__ Tt,
                                                              const unsigned long long* __restrict__ mask,
                                                              const uint32_t* __restrict__ sigma_inv, int m, int K,
-                                                             uint32_t* Mout, int64_t out_rs, int64_t out_cs, ModP M) {
+                                                             uint32_t* Mout, int64_t out_rs, int64_t out_cs,
+                                                             int64_t out_bs, ModP M) {
   extern __shared__ __align__(16) uint32_t bb_smem[];
+  // matrix blockIdx.y of the batch
+  Tt += (int64_t)blockIdx.y * K * m * m;
+  mask += (int64_t)blockIdx.y * K;
+  sigma_inv += (int64_t)blockIdx.y * m;
+  Mout += (int64_t)blockIdx.y * out_bs;
   const int S = m + 1;            // row stride of V
   const int TS = leaf_tstride(m); // row stride of the slot-ordered transform
   const int VS = ((K + 1) * S + 3) & ~3;  // words per V buffer (16-byte multiple)
@@ -1189,99 +1310,138 @@ struct Pm {
   rr_ctx* ctx = nullptr;
   cudaStream_t s = nullptr;
   int m = 0, n = 0;
+  int nb = 1;  // generators solved together (same b, d, p)
   uint32_t p = 0;
   ModP M{};
   int K = 0;
   bool use_ntt = false;
   int64_t nmax = 0;
   DevBuf<uint32_t> tw, tws, twi, twis;
-  DevBuf<uint32_t> FA, FB, FC;
-  DevBuf<uint32_t> Tt;                 // leaf transforms of one block [K][m][m]
-  DevBuf<unsigned long long> leafmask; // [K]
-  DevBuf<uint32_t> sigma_inv;          // [m]
-  DevBuf<int64_t> delta;
+  DevBuf<uint32_t> FA, FB, FC;          // [nb][m*m][nmax]
+  DevBuf<uint32_t> Tt;                  // leaf transforms of one block [nb][K][m][m]
+  DevBuf<unsigned long long> leafmask;  // [nb][K]
+  DevBuf<uint32_t> sigma_inv;           // [nb][m]
+  DevBuf<int64_t> delta;                // [nb][m]
   DevBuf<int> status;
   int64_t cs = 0;                      // residual coefficient stride of the leaves kernel (words)
   int fold4 = 0;
   bool mma = false;                    // tensor-core leaves kernel (b <= 16)
-  // per recursion depth: MM, GG, MMM
+  // per recursion depth: MM, GG, MMM ([nb] each)
   std::vector<std::unique_ptr<DevBuf<uint32_t>>> bufs;
   Twiddles fwd() const { return Twiddles{tw.ptr, tws.ptr, nmax}; }
   Twiddles inv() const { return Twiddles{twi.ptr, twis.ptr, nmax}; }
 };
 
-int ntt_forward(Pm& P, uint32_t* a, int64_t N, int64_t npoly, const uint32_t* src, int src_cols, int64_t src_rs,
-                int64_t src_cs, int64_t src_len) {
-  const int T = (int)std::min<int64_t>(N, kNttBlock);
-  const int threads = std::min(512, std::max(32, T / 2));
+// A strided polynomial matrix of every generator of the batch: entry (i, j)
+// of generator z starts at p + z * bs + i * rs + j * cs.
+struct MatView {
+  uint32_t* p;
+  int64_t rs, cs, bs;
+  PolyView polys(int cols, int rows) const { return PolyView{p, cols, rows * cols, rs, cs, bs}; }
+};
+
+// NTTs of the npb polynomials of each of the nb generators in src (zero
+// padded to N) into a (dense, [nb * npb][N]).
+// Launch shape of the shared-memory NTT kernels for span T over nblocks blocks.
+struct NttShape {
+  int logT, G, threads;
+  unsigned grid;
+  size_t smem;
+};
+NttShape ntt_shape(int64_t T, int64_t nblocks) {
+  NttShape sh;
+  sh.logT = 0;
+  while ((1ll << sh.logT) < T) ++sh.logT;
+  sh.G = T >= kNttGroup ? 1 : (int)(kNttGroup / T);
+  sh.threads = (int)std::min<int64_t>(512, std::max<int64_t>(32, sh.G * T / 2));
+  sh.grid = (unsigned)((nblocks + sh.G - 1) / sh.G);
+  sh.smem = (size_t)(sh.G * T + T) * 4;
+  return sh;
+}
+
+int ntt_forward(Pm& P, uint32_t* a, int64_t N, PolyView src, int64_t src_len) {
+  const int64_t npoly = (int64_t)P.nb * src.npb;
+  const int64_t T = std::min<int64_t>(N, kNttBlock);
   if (N <= kNttBlock) {
-    ntt_fwd_smem_kernel<<<(unsigned)npoly, threads, 0, P.s>>>(a, N, T, src, src_cols, src_rs, src_cs, src_len, P.fwd(), P.p);
+    const NttShape sh = ntt_shape(T, npoly);
+    ntt_fwd_smem_kernel<<<sh.grid, sh.threads, sh.smem, P.s>>>(a, N, sh.logT, npoly, src, src_len, P.fwd(), P.p);
     RR_CUDA(cudaGetLastError());
     return RR_OK;
   }
-  pad_copy_kernel<<<grid_for(npoly * N), 256, 0, P.s>>>(a, N, npoly, src, src_cols, src_rs, src_cs, src_len);
+  pad_copy_kernel<<<grid_for(npoly * N), 256, 0, P.s>>>(a, N, npoly, src, src_len);
   RR_CUDA(cudaGetLastError());
   for (int64_t len = N; len > kNttBlock; len >>= 1) {
     ntt_fwd_stage_kernel<<<grid_for(npoly * N / 2), 256, 0, P.s>>>(a, N, npoly, len, P.fwd(), P.p);
     RR_CUDA(cudaGetLastError());
   }
-  ntt_fwd_smem_kernel<<<(unsigned)(npoly * (N / T)), threads, 0, P.s>>>(a, N, T, nullptr, 1, 0, 0, 0, P.fwd(), P.p);
+  const PolyView none{nullptr, 1, 1, 0, 0, 0};
+  const NttShape sh = ntt_shape(T, npoly * (N / T));
+  ntt_fwd_smem_kernel<<<sh.grid, sh.threads, sh.smem, P.s>>>(a, N, sh.logT, npoly * (N / T), none, 0, P.fwd(), P.p);
   RR_CUDA(cudaGetLastError());
   return RR_OK;
 }
 
-int ntt_inverse(Pm& P, uint32_t* a, int64_t N, int64_t npoly, uint32_t* dst, int dst_cols, int64_t dst_rs, int64_t dst_cs,
-                int64_t lo, int64_t cnt) {
-  const int T = (int)std::min<int64_t>(N, kNttBlock);
-  const int threads = std::min(512, std::max(32, T / 2));
+// Inverse NTTs of a ([nb * npb][N]); coefficients [lo, lo + cnt), scaled by
+// N^{-1}, go to dst.
+int ntt_inverse(Pm& P, uint32_t* a, int64_t N, PolyView dst, int64_t lo, int64_t cnt) {
+  const int64_t npoly = (int64_t)P.nb * dst.npb;
+  const int64_t T = std::min<int64_t>(N, kNttBlock);
   const uint32_t ninv = host_invmod((uint32_t)(N % P.p), P.p);
   const uint32_t ninv_s = (uint32_t)(((uint64_t)ninv << 32) / P.p);
   if (N <= kNttBlock) {
-    ntt_inv_smem_kernel<<<(unsigned)npoly, threads, 0, P.s>>>(a, N, T, dst, dst_cols, dst_rs, dst_cs, lo, cnt, ninv, ninv_s,
-                                                             P.inv(), P.p);
+    const NttShape sh = ntt_shape(T, npoly);
+    ntt_inv_smem_kernel<<<sh.grid, sh.threads, sh.smem, P.s>>>(a, N, sh.logT, npoly, dst, lo, cnt, ninv, ninv_s,
+                                                               P.inv(), P.p);
     RR_CUDA(cudaGetLastError());
     return RR_OK;
   }
-  ntt_inv_smem_kernel<<<(unsigned)(npoly * (N / T)), threads, 0, P.s>>>(a, N, T, nullptr, 1, 0, 0, 0, 0, 0, 0, P.inv(), P.p);
+  const PolyView none{nullptr, 1, 1, 0, 0, 0};
+  const NttShape sh = ntt_shape(T, npoly * (N / T));
+  ntt_inv_smem_kernel<<<sh.grid, sh.threads, sh.smem, P.s>>>(a, N, sh.logT, npoly * (N / T), none, 0, 0, 0, 0,
+                                                             P.inv(), P.p);
   RR_CUDA(cudaGetLastError());
   for (int64_t len = 2 * kNttBlock; len <= N; len <<= 1) {
     ntt_inv_stage_kernel<<<grid_for(npoly * N / 2), 256, 0, P.s>>>(a, N, npoly, len, P.inv(), P.p);
     RR_CUDA(cudaGetLastError());
   }
-  extract_scale_kernel<<<grid_for(npoly * cnt), 256, 0, P.s>>>(a, N, npoly, dst, dst_cols, dst_rs, dst_cs, lo, cnt, ninv,
-                                                              ninv_s, P.p);
+  extract_scale_kernel<<<grid_for(npoly * cnt), 256, 0, P.s>>>(a, N, npoly, dst, lo, cnt, ninv, ninv_s, P.p);
   RR_CUDA(cudaGetLastError());
   return RR_OK;
 }
 
-// dst[i][j][0..cnt) = coefficients [lo, lo+cnt) of A * B, where
-// A is mA x r with la coefficients (strides a_rs, a_cs) and B is r x k with
-// lb coefficients (strides b_rs, b_cs); dst has strides d_rs, d_cs.
-int poly_mat_mul(Pm& P, const uint32_t* A, int mA, int r, int64_t la, int64_t a_rs, int64_t a_cs, const uint32_t* B,
-                 int k, int64_t lb, int64_t b_rs, int64_t b_cs, uint32_t* dst, int64_t d_rs, int64_t d_cs, int64_t lo,
+// dst[i][j][0..cnt) = coefficients [lo, lo+cnt) of A * B for every generator
+// of the batch, where A is mA x r with la coefficients and B is r x k with lb
+// coefficients.
+int poly_mat_mul(Pm& P, MatView A, int mA, int r, int64_t la, MatView B, int k, int64_t lb, MatView dst, int64_t lo,
                  int64_t cnt) {
   int64_t N = 1;
   while (N < la + lb - 1) N <<= 1;
   if (!P.use_ntt) {
-    schoolbook_kernel<<<grid_for((int64_t)mA * k * cnt), 256, 0, P.s>>>(A, mA, r, la, a_rs, a_cs, B, k, lb, b_rs, b_cs,
-                                                                        dst, d_rs, d_cs, lo, cnt, P.M);
+    schoolbook_kernel<<<grid_for((int64_t)P.nb * mA * k * cnt), 256, 0, P.s>>>(
+        A.p, mA, r, la, A.rs, A.cs, A.bs, B.p, k, lb, B.rs, B.cs, B.bs, dst.p, dst.rs, dst.cs, dst.bs, lo, cnt, P.nb,
+        P.M);
     RR_CUDA(cudaGetLastError());
     return RR_OK;
   }
   if (N > P.nmax) return fail(RR_EINVAL, "internal: NTT length %lld exceeds table %lld", (long long)N, (long long)P.nmax);
-  RR_TRY(ntt_forward(P, P.FA.ptr, N, (int64_t)mA * r, A, r, a_rs, a_cs, la));
-  RR_TRY(ntt_forward(P, P.FB.ptr, N, (int64_t)r * k, B, k, b_rs, b_cs, lb));
-  pointwise_kernel<<<grid_for((int64_t)mA * k * N), 256, 0, P.s>>>(P.FA.ptr, P.FB.ptr, P.FC.ptr, mA, r, k, N, P.M);
+  RR_TRY(ntt_forward(P, P.FA.ptr, N, A.polys(r, mA), la));
+  RR_TRY(ntt_forward(P, P.FB.ptr, N, B.polys(k, r), lb));
+  if (mA % 4 == 0 && k % 4 == 0)
+    pointwise_kernel<<<grid_for((int64_t)P.nb * (mA / 4) * (k / 4) * N), 256, 0, P.s>>>(
+        P.FA.ptr, P.FB.ptr, P.FC.ptr, mA, r, k, N, P.nb, P.fold4 ? 3 : 1, P.M);
+  else
+    pointwise1_kernel<<<grid_for((int64_t)P.nb * mA * k * N), 256, 0, P.s>>>(P.FA.ptr, P.FB.ptr, P.FC.ptr, mA, r, k, N,
+                                                                              P.nb, P.M);
   RR_CUDA(cudaGetLastError());
-  return ntt_inverse(P, P.FC.ptr, N, (int64_t)mA * k, dst, k, d_rs, d_cs, lo, cnt);
+  return ntt_inverse(P, P.FC.ptr, N, dst.polys(k, mA), lo, cnt);
 }
 
-int run_base(Pm& P, const uint32_t* G, int64_t g_rs, int64_t g_cs, int nleaves, uint32_t* Mout, int64_t o_rs,
-             int64_t o_cs) {
+int run_base(Pm& P, MatView G, int nleaves, MatView Mout) {
   LeafParams L;
-  L.G = G;
-  L.g_rs = g_rs;
-  L.g_cs = g_cs;
+  L.G = G.p;
+  L.g_rs = G.rs;
+  L.g_cs = G.cs;
+  L.g_bs = G.bs;
   L.m = P.m;
   L.n = P.n;
   L.K = nleaves;
@@ -1292,25 +1452,29 @@ int run_base(Pm& P, const uint32_t* G, int64_t g_rs, int64_t g_cs, int nleaves, 
   L.sigma_inv = P.sigma_inv.ptr;
   L.M = P.M;
   L.status = P.status.ptr;
+  const unsigned nb = (unsigned)P.nb;
   if (P.mma) {
-    pm_leaves_mma_kernel<<<1, kLeafThreads, leaves_mma_smem_bytes(P.m, P.n, nleaves), P.s>>>(L);
+    pm_leaves_mma_kernel<<<nb, kLeafThreads, leaves_mma_smem_bytes(P.m, P.n, nleaves), P.s>>>(L);
   } else if (P.n % 4 == 0) {
     const size_t smem = leaves_smem_bytes(P.m, P.n, nleaves, P.cs);
-    if (P.fold4) pm_leaves_kernel<4, 4><<<1, kLeafThreads, smem, P.s>>>(L);
-    else pm_leaves_kernel<4, 2><<<1, kLeafThreads, smem, P.s>>>(L);
+    if (P.fold4) pm_leaves_kernel<4, 4><<<nb, kLeafThreads, smem, P.s>>>(L);
+    else pm_leaves_kernel<4, 2><<<nb, kLeafThreads, smem, P.s>>>(L);
   } else {
     const size_t smem = leaves_smem_bytes(P.m, P.n, nleaves, P.cs);
-    if (P.fold4) pm_leaves_kernel<1, 4><<<1, kLeafThreads, smem, P.s>>>(L);
-    else pm_leaves_kernel<1, 2><<<1, kLeafThreads, smem, P.s>>>(L);
+    if (P.fold4) pm_leaves_kernel<1, 4><<<nb, kLeafThreads, smem, P.s>>>(L);
+    else pm_leaves_kernel<1, 2><<<nb, kLeafThreads, smem, P.s>>>(L);
   }
   RR_CUDA(cudaGetLastError());
+  // the leaves kernel indexes its transforms with the block's own K; the
+  // block basis reads them with the same K
   const size_t bsm = block_basis_smem_bytes(P.m, nleaves);
+  const dim3 grid((unsigned)P.m, nb);
   if (P.fold4)
-    pm_block_basis_kernel<4><<<P.m, 256, bsm, P.s>>>(P.Tt.ptr, P.leafmask.ptr, P.sigma_inv.ptr, P.m, nleaves, Mout,
-                                                     o_rs, o_cs, P.M);
+    pm_block_basis_kernel<4><<<grid, 256, bsm, P.s>>>(P.Tt.ptr, P.leafmask.ptr, P.sigma_inv.ptr, P.m, nleaves, Mout.p,
+                                                      Mout.rs, Mout.cs, Mout.bs, P.M);
   else
-    pm_block_basis_kernel<2><<<P.m, 256, bsm, P.s>>>(P.Tt.ptr, P.leafmask.ptr, P.sigma_inv.ptr, P.m, nleaves, Mout,
-                                                     o_rs, o_cs, P.M);
+    pm_block_basis_kernel<2><<<grid, 256, bsm, P.s>>>(P.Tt.ptr, P.leafmask.ptr, P.sigma_inv.ptr, P.m, nleaves, Mout.p,
+                                                      Mout.rs, Mout.cs, Mout.bs, P.M);
   RR_CUDA(cudaGetLastError());
   return RR_OK;
 }
@@ -1349,32 +1513,47 @@ int set_base_smem_limit(size_t bytes) {
   return RR_OK;
 }
 
-// _PM_Basis (src/sigma_basis.rs:190-219) on G (m x n, strides g_rs/g_cs,
-// coefficients [0, d] used); M_out receives m x m x (d+1) (strides o_rs/o_cs).
-int pm_rec(Pm& P, const uint32_t* G, int64_t g_rs, int64_t g_cs, int64_t d, int depth, uint32_t* Mo, int64_t o_rs,
-           int64_t o_cs) {
-  if (d <= P.K) return run_base(P, G, g_rs, g_cs, (int)d, Mo, o_rs, o_cs);
+// _PM_Basis (src/sigma_basis.rs:190-219) on G (m x n, coefficients [0, d]
+// used) for every generator of the batch; Mo receives m x m x (d+1).
+int pm_rec(Pm& P, MatView G, int64_t d, int depth, MatView Mo) {
+  if (d <= P.K) return run_base(P, G, (int)d, Mo);
   const int m = P.m, n = P.n;
   const int64_t h = d / 2;
-  uint32_t* MM = P.bufs[3 * depth + 0]->ptr;   // m x m x (h+1)
-  uint32_t* GG = P.bufs[3 * depth + 1]->ptr;   // m x n x (h+1)
-  uint32_t* MMM = P.bufs[3 * depth + 2]->ptr;  // m x m x (h+1)
   const int64_t hl = h + 1;
-  RR_TRY(pm_rec(P, G, g_rs, g_cs, h, depth + 1, MM, (int64_t)m * hl, hl));
+  const MatView MM{P.bufs[3 * depth + 0]->ptr, (int64_t)m * hl, hl, (int64_t)m * m * hl};   // m x m x (h+1)
+  const MatView GG{P.bufs[3 * depth + 1]->ptr, (int64_t)n * hl, hl, (int64_t)m * n * hl};   // m x n x (h+1)
+  const MatView MMM{P.bufs[3 * depth + 2]->ptr, (int64_t)m * hl, hl, (int64_t)m * m * hl};  // m x m x (h+1)
+  RR_TRY(pm_rec(P, G, h, depth + 1, MM));
   // GG = (MM * G)[h .. d]   (poly_mat_mul_red_adaptive(MM, G, p, 0, d+1) + shift_trunc_in(h, h))
-  RR_TRY(poly_mat_mul(P, MM, m, m, hl, (int64_t)m * hl, hl, G, n, d + 1, g_rs, g_cs, GG, (int64_t)n * hl, hl, h, hl));
-  RR_TRY(pm_rec(P, GG, (int64_t)n * hl, hl, h, depth + 1, MMM, (int64_t)m * hl, hl));
+  RR_TRY(poly_mat_mul(P, MM, m, m, hl, G, n, d + 1, GG, h, hl));
+  RR_TRY(pm_rec(P, GG, h, depth + 1, MMM));
   // M = MMM * MM
-  return poly_mat_mul(P, MMM, m, m, hl, (int64_t)m * hl, hl, MM, m, hl, (int64_t)m * hl, hl, Mo, o_rs, o_cs, 0, d + 1);
+  return poly_mat_mul(P, MMM, m, m, hl, MM, m, hl, Mo, 0, d + 1);
 }
 
 }  // namespace
 
-int pm_basis_device(rr_ctx* ctx, const uint32_t* seq, int64_t seq_stride, int b, int64_t nlen, int64_t d, uint32_t p,
-                    uint32_t* Mh, int64_t* deltah) {
+// Device bytes the batched generator holds per generator of degree d and width b.
+size_t pm_workspace_bytes(int b, int64_t d) {
+  const size_t m = 2 * (size_t)b, n = (size_t)b;
+  int64_t nmax = 1;
+  while (nmax < d + d / 2 + 1) nmax <<= 1;
+  size_t bytes = 3 * m * m * (size_t)nmax * 4;               // NTT workspace
+  for (int64_t dd = d; dd > 1; dd /= 2) bytes += (2 * m * m + m * n) * (size_t)(dd / 2 + 1) * 4;  // per depth
+  bytes += (m * n + m * m) * (size_t)(d + 1) * 4 + (size_t)b * (b + 1) / 2 * (size_t)(d + 1) * 4;  // G, Mo, seq
+  bytes += 64 * m * m * 4;                                    // leaf transforms
+  return bytes;
+}
+
+// PM-basis of nb generators with the same b, d and p, solved in lockstep: one
+// leaf-kernel CTA per generator, one launch per NTT / product step for all.
+int pm_basis_batch_device(rr_ctx* ctx, int nb, const uint32_t* const* seqs, const int64_t* seq_strides, int b,
+                          int64_t d, uint32_t p, uint32_t* const* Mh, int64_t* const* deltah) {
+  if (nb < 1) return RR_OK;
   Pm P;
   P.ctx = ctx;
   P.s = ctx->stream;
+  P.nb = nb;
   P.m = 2 * b;
   P.n = b;
   P.p = p;
@@ -1420,10 +1599,10 @@ int pm_basis_device(rr_ctx* ctx, const uint32_t* seq, int64_t seq_stride, int b,
     RR_CUDA(cudaMemcpyAsync(P.tws.ptr, ts.data(), ts.size() * 4, cudaMemcpyHostToDevice, P.s));
     RR_CUDA(cudaMemcpyAsync(P.twi.ptr, ti.data(), ti.size() * 4, cudaMemcpyHostToDevice, P.s));
     RR_CUDA(cudaMemcpyAsync(P.twis.ptr, tis.data(), tis.size() * 4, cudaMemcpyHostToDevice, P.s));
-    RR_TRY(P.FA.alloc_async((size_t)m * m * nmax, P.s));
-    RR_TRY(P.FB.alloc_async((size_t)m * m * nmax, P.s));
-    RR_TRY(P.FC.alloc_async((size_t)m * m * nmax, P.s));
-    RR_CUDA(cudaStreamSynchronize(P.s));
+    RR_TRY(P.FA.alloc_async((size_t)nb * m * m * nmax, P.s));
+    RR_TRY(P.FB.alloc_async((size_t)nb * m * m * nmax, P.s));
+    RR_TRY(P.FC.alloc_async((size_t)nb * m * m * nmax, P.s));
+    RR_CUDA(cudaStreamSynchronize(P.s));  // the host tables die at scope end
   }
   // per-depth buffers
   {
@@ -1432,41 +1611,56 @@ int pm_basis_device(rr_ctx* ctx, const uint32_t* seq, int64_t seq_stride, int b,
       const int64_t hl = dd / 2 + 1;
       for (int q = 0; q < 3; ++q) {
         P.bufs.emplace_back(new DevBuf<uint32_t>());
-        RR_TRY(P.bufs.back()->alloc_async((size_t)m * (q == 1 ? n : m) * hl, P.s));
+        RR_TRY(P.bufs.back()->alloc_async((size_t)nb * m * (q == 1 ? n : m) * hl, P.s));
       }
     }
   }
-  RR_TRY(P.delta.alloc_async(m, P.s));
+  RR_TRY(P.delta.alloc_async((size_t)nb * m, P.s));
   RR_TRY(P.status.alloc_async(1, P.s));
-  RR_TRY(P.Tt.alloc_async((size_t)P.K * m * m, P.s));
-  RR_TRY(P.leafmask.alloc_async((size_t)P.K, P.s));
-  RR_TRY(P.sigma_inv.alloc_async((size_t)m, P.s));
-  RR_CUDA(cudaMemsetAsync(P.delta.ptr, 0, m * sizeof(int64_t), P.s));
+  RR_TRY(P.Tt.alloc_async((size_t)nb * P.K * m * m, P.s));
+  RR_TRY(P.leafmask.alloc_async((size_t)nb * P.K, P.s));
+  RR_TRY(P.sigma_inv.alloc_async((size_t)nb * m, P.s));
+  RR_CUDA(cudaMemsetAsync(P.delta.ptr, 0, (size_t)nb * m * sizeof(int64_t), P.s));
   RR_CUDA(cudaMemsetAsync(P.status.ptr, 0, sizeof(int), P.s));
   // the limits are per kernel, shared by every caller in the process (the
   // batched engine runs generators on several threads): always the budget,
   // never this call's size, so a concurrent smaller call cannot lower them
   if (leaves_smem > kBaseSmemBudget) return fail(RR_EUNSUPPORTED, "leaf block needs %zu bytes of shared memory", leaves_smem);
   RR_TRY(set_leaves_smem_limit(kBaseSmemBudget, block_basis_smem_bytes(64, 64)));
-  // G = [S; I], coefficients [0, d]
+  // G = [S; I], coefficients [0, d], one after the other
   DevBuf<uint32_t> dseq, G;
   const int np = b * (b + 1) / 2;
   const int64_t glen = d + 1;
-  RR_TRY(dseq.alloc_async((size_t)np * glen, P.s));
-  RR_CUDA(cudaMemcpy2DAsync(dseq.ptr, glen * 4, seq, seq_stride * 4, glen * 4, np, cudaMemcpyHostToDevice, P.s));
-  RR_TRY(G.alloc_async((size_t)m * n * glen, P.s));
-  build_G_kernel<<<grid_for((int64_t)m * n * glen), 256, 0, P.s>>>(dseq.ptr, glen, b, glen, G.ptr, p);
-  RR_CUDA(cudaGetLastError());
+  RR_TRY(dseq.alloc_async((size_t)nb * np * glen, P.s));
+  RR_TRY(G.alloc_async((size_t)nb * m * n * glen, P.s));
+  for (int z = 0; z < nb; ++z) {
+    uint32_t* dz = dseq.ptr + (size_t)z * np * glen;
+    RR_CUDA(cudaMemcpy2DAsync(dz, glen * 4, seqs[z], seq_strides[z] * 4, glen * 4, np, cudaMemcpyHostToDevice, P.s));
+    build_G_kernel<<<grid_for((int64_t)m * n * glen), 256, 0, P.s>>>(dz, glen, b, glen, G.ptr + (size_t)z * m * n * glen,
+                                                                     p);
+    RR_CUDA(cudaGetLastError());
+  }
   DevBuf<uint32_t> Mo;
-  RR_TRY(Mo.alloc_async((size_t)m * m * (d + 1), P.s));
-  RR_TRY(pm_rec(P, G.ptr, (int64_t)n * glen, glen, d, 0, Mo.ptr, (int64_t)m * (d + 1), d + 1));
+  RR_TRY(Mo.alloc_async((size_t)nb * m * m * (d + 1), P.s));
+  const MatView Gv{G.ptr, (int64_t)n * glen, glen, (int64_t)m * n * glen};
+  const MatView Mv{Mo.ptr, (int64_t)m * (d + 1), d + 1, (int64_t)m * m * (d + 1)};
+  RR_TRY(pm_rec(P, Gv, d, 0, Mv));
   int status = 0;
-  RR_CUDA(cudaMemcpyAsync(Mh, Mo.ptr, Mo.bytes(), cudaMemcpyDeviceToHost, P.s));
-  RR_CUDA(cudaMemcpyAsync(deltah, P.delta.ptr, m * sizeof(int64_t), cudaMemcpyDeviceToHost, P.s));
+  for (int z = 0; z < nb; ++z) {
+    RR_CUDA(cudaMemcpyAsync(Mh[z], Mo.ptr + (size_t)z * m * m * (d + 1), (size_t)m * m * (d + 1) * 4,
+                            cudaMemcpyDeviceToHost, P.s));
+    RR_CUDA(cudaMemcpyAsync(deltah[z], P.delta.ptr + (size_t)z * m, m * sizeof(int64_t), cudaMemcpyDeviceToHost, P.s));
+  }
   RR_CUDA(cudaMemcpyAsync(&status, P.status.ptr, sizeof(int), cudaMemcpyDeviceToHost, P.s));
   RR_CUDA(cudaStreamSynchronize(P.s));
   if (status) return fail(RR_ECUDA, "PM-basis device status %d (zero row scale)", status);
   return RR_OK;
+}
+
+int pm_basis_device(rr_ctx* ctx, const uint32_t* seq, int64_t seq_stride, int b, int64_t nlen, int64_t d, uint32_t p,
+                    uint32_t* Mh, int64_t* deltah) {
+  (void)nlen;
+  return pm_basis_batch_device(ctx, 1, &seq, &seq_stride, b, d, p, &Mh, &deltah);
 }
 
 // ---------------------------------------------------------------- no-allocation variant

@@ -169,5 +169,11 @@ int matrix_build(rr_ctx* ctx, int64_t m, int64_t n, const int64_t* rowptr, const
 // PM-basis on the device; M (host) [2b][2b][d+1], delta (host) [2b].
 int pm_basis_device(rr_ctx* ctx, const uint32_t* seq, int64_t seq_stride, int b, int64_t nlen, int64_t d,
                     uint32_t p, uint32_t* M, int64_t* delta);
+// The same for nb generators with equal b, d and p in lockstep (one launch per
+// step for all); seqs[z] is [b(b+1)/2][seq_strides[z]], Mh[z] and deltah[z] as above.
+int pm_basis_batch_device(rr_ctx* ctx, int nb, const uint32_t* const* seqs, const int64_t* seq_strides, int b,
+                          int64_t d, uint32_t p, uint32_t* const* Mh, int64_t* const* deltah);
+// Device bytes pm_basis_batch_device needs per generator.
+size_t pm_workspace_bytes(int b, int64_t d);
 int rank_from_basis_host(const uint32_t* M, const int64_t* delta, int b, int64_t len, uint32_t p, int64_t* rank);
 }  // namespace rr

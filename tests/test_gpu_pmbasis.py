@@ -68,3 +68,29 @@ def test_rank_known_by_construction(ctx, b):
     V = synth.random_vectors(b, n, P, 9)
     r_orc, _, _, _ = oracle.rank_pipeline(rowptr, col, val, m, n, P, rp, cp, V)
     assert rr.block_wiedemann_rank(a, b, P, row_precond=rp, col_precond=cp, v=V, ctx=ctx) == r_orc == dense
+
+
+@pytest.mark.parametrize("b,d,count", [(2, 64, 3), (8, 256, 5), (16, 128, 4), (16, 64, 1), (3, 40, 2), (32, 16, 3)])
+def test_batched_pm_basis_equals_single(ctx, b, d, count):
+    """rr_pm_basis_batch (generators in lockstep) gives each sequence the
+    generator rr_pm_basis gives it alone, bit for bit."""
+    rng = np.random.default_rng(b * 31 + d)
+    dd = 1 << (d - 1).bit_length()
+    seqs = [rng.integers(0, P, size=(b * (b + 1) // 2, dd + 2)).astype(np.uint32) for _ in range(count)]
+    got = rr.PM_Basis_batch(seqs, d, P, ctx)
+    for s, (M, delta) in zip(seqs, got):
+        M1, d1 = rr.PM_Basis(s, d, P, ctx)
+        assert np.array_equal(M, M1) and np.array_equal(delta, d1)
+
+
+def test_batched_pm_basis_small_prime_golden(ctx, golden):
+    """The batched path on the reference's golden cases at p = 3323 (direct products)."""
+    z = golden("pm_basis_ref.npz")
+    by_shape = {}
+    for i in range(int(z["count"])):
+        b, d, _ = (int(x) for x in z[f"c{i}_meta"])
+        by_shape.setdefault((b, d, z[f"c{i}_seq"].shape), []).append(i)
+    for (b, d, _), idx in by_shape.items():
+        got = rr.PM_Basis_batch([z[f"c{i}_seq"] for i in idx], d, 3323, ctx)
+        for i, (M, delta) in zip(idx, got):
+            assert np.array_equal(M, z[f"c{i}_M"]) and np.array_equal(delta, z[f"c{i}_delta"]), i
