@@ -13,10 +13,12 @@
 //              every running request, two chunks in flight per request, so
 //              the Krylov steps of different requests interleave on the
 //              lanes and overlap on the device
-//   solving -> once its sequence is complete a worker thread copies it out,
-//              runs the generator (rr_pm_basis) on a stream of its own and
-//              reads off the rank (rr_rank_from_basis), then frees the
-//              request's device memory, which admits the next requests
+//   solving -> once its sequence is complete a worker thread copies it out
+//              and solves the generator on a stream of its own, together
+//              with the other complete requests of the same sequence length
+//              (one batched PM-basis, generators in lockstep), reads off the
+//              rank (rr_rank_from_basis) and frees the request's device
+//              memory, which admits the next requests
 //   done
 //
 // Every request follows exactly the path of rr_rank on the same inputs
@@ -41,6 +43,8 @@ namespace {
 using Clock = std::chrono::steady_clock;
 
 enum ReqState { kQueued, kLoading, kRunning, kSolving, kDone, kFailed };
+
+constexpr int kMaxSolveBatch = 32;  // generators solved together by one worker
 
 struct Request {
   uint64_t id = 0;
@@ -98,7 +102,8 @@ struct rr_server_s {
   std::condition_variable cv_sched, cv_work, cv_done;
   std::map<uint64_t, std::unique_ptr<Request>> reqs;
   std::deque<uint64_t> queue;      // submitted, not yet admitted
-  std::deque<uint64_t> tasks;      // for the workers: loading or solving requests
+  std::deque<uint64_t> tasks;      // for the workers: requests to load
+  std::deque<uint64_t> solve_q;    // for the workers: requests whose sequences are complete
   std::vector<uint64_t> running;   // for the scheduler
   size_t used = 0;
   int active = 0;
@@ -162,30 +167,47 @@ struct rr_server_s {
     return RR_OK;
   }
 
-  // Worker: sequence -> generator -> rank, on the worker's own context.
-  int solve(Request& r, rr_ctx* wctx) {
-    const int b = cfg.b, np = b * (b + 1) / 2;
-    const int64_t L = 1 + 2 * r.apps_total;
+  // Worker: sequences -> generators (in lockstep) -> ranks, on the worker's
+  // own context, for requests of equal sequence length.
+  int solve(std::vector<Request*>& rs, rr_ctx* wctx) {
+    const int b = cfg.b, np = b * (b + 1) / 2, cnt = (int)rs.size();
+    const int64_t L = 1 + 2 * rs[0]->apps_total;
     RR_CUDA(cudaSetDevice(device));
     // every chunk's event has completed (the scheduler saw them), so the
-    // sequence is final in device memory
-    std::vector<uint32_t> raw((size_t)L * np), seq((size_t)np * L);
-    RR_CUDA(cudaMemcpyAsync(raw.data(), r.kr->S.ptr, raw.size() * 4, cudaMemcpyDeviceToHost,
-                            (cudaStream_t)rr_ctx_stream(wctx)));
-    RR_CUDA(cudaStreamSynchronize((cudaStream_t)rr_ctx_stream(wctx)));
-    for (int64_t t = 0; t < L; ++t)
-      for (int q = 0; q < np; ++q) seq[(size_t)q * L + t] = raw[(size_t)t * np + q];
-    rr_krylov_destroy(r.kr);
-    r.kr = nullptr;
-    rr_matrix_destroy(r.mat);
-    r.mat = nullptr;
+    // sequences are final in device memory
+    std::vector<uint32_t> raw((size_t)L * np);
+    std::vector<std::vector<uint32_t>> seq(cnt);
+    for (int z = 0; z < cnt; ++z) {
+      RR_CUDA(cudaMemcpyAsync(raw.data(), rs[z]->kr->S.ptr, raw.size() * 4, cudaMemcpyDeviceToHost,
+                              (cudaStream_t)rr_ctx_stream(wctx)));
+      RR_CUDA(cudaStreamSynchronize((cudaStream_t)rr_ctx_stream(wctx)));
+      seq[z].resize((size_t)np * L);
+      for (int64_t t = 0; t < L; ++t)
+        for (int q = 0; q < np; ++q) seq[z][(size_t)q * L + t] = raw[(size_t)t * np + q];
+      rr_krylov_destroy(rs[z]->kr);
+      rs[z]->kr = nullptr;
+      rr_matrix_destroy(rs[z]->mat);
+      rs[z]->mat = nullptr;
+    }
     int64_t d = 1;  // src/main.rs:599-603
     while (d <= L) d *= 2;
     d /= 2;
-    std::vector<uint32_t> M((size_t)(2 * b) * (2 * b) * (d + 1));
-    std::vector<int64_t> delta(2 * b);
-    RR_TRY(rr_pm_basis(wctx, seq.data(), L, b, L, d, cfg.p, M.data(), delta.data()));
-    return rr_rank_from_basis(M.data(), delta.data(), b, d + 1, cfg.p, &r.rank);
+    std::vector<std::vector<uint32_t>> M(cnt);
+    std::vector<std::vector<int64_t>> delta(cnt);
+    std::vector<const uint32_t*> sp(cnt);
+    std::vector<uint32_t*> mp(cnt);
+    std::vector<int64_t*> dp(cnt);
+    std::vector<int64_t> strides(cnt, L);
+    for (int z = 0; z < cnt; ++z) {
+      M[z].resize((size_t)(2 * b) * (2 * b) * (d + 1));
+      delta[z].resize(2 * b);
+      sp[z] = seq[z].data();
+      mp[z] = M[z].data();
+      dp[z] = delta[z].data();
+    }
+    RR_TRY(rr::pm_basis_batch_device(wctx, cnt, sp.data(), strides.data(), b, d, cfg.p, mp.data(), dp.data()));
+    for (int z = 0; z < cnt; ++z) RR_TRY(rr_rank_from_basis(M[z].data(), delta[z].data(), b, d + 1, cfg.p, &rs[z]->rank));
+    return RR_OK;
   }
 
   void release(Request& r) {
@@ -206,39 +228,52 @@ struct rr_server_s {
     const int wrc = rr_ctx_create(device, &wctx);
     const std::string werr = wrc == RR_OK ? std::string() : std::string(rr_last_error());
     for (;;) {
-      uint64_t id;
+      std::vector<Request*> batch;
+      bool loading = false;
       {
         std::unique_lock<std::mutex> lk(mu);
-        cv_work.wait(lk, [&] { return stop || !tasks.empty(); });
+        cv_work.wait(lk, [&] { return stop || !tasks.empty() || !solve_q.empty(); });
         if (stop) break;
-        id = tasks.front();
-        tasks.pop_front();
-      }
-      Request* r;
-      ReqState st;
-      {
-        std::lock_guard<std::mutex> lk(mu);
-        r = reqs[id].get();
-        st = r->state;
+        if (!tasks.empty()) {  // loads first: they keep the Krylov lanes busy
+          batch.push_back(reqs[tasks.front()].get());
+          tasks.pop_front();
+          loading = true;
+        } else {
+          // this request and every other complete one of the same length
+          Request* r0 = reqs[solve_q.front()].get();
+          solve_q.pop_front();
+          batch.push_back(r0);
+          for (auto it = solve_q.begin(); it != solve_q.end() && (int)batch.size() < kMaxSolveBatch;) {
+            Request* r = reqs[*it].get();
+            if (r->apps_total == r0->apps_total) {
+              batch.push_back(r);
+              it = solve_q.erase(it);
+            } else {
+              ++it;
+            }
+          }
+        }
       }
       int rc = wrc;
       std::string err = werr;
       if (rc == RR_OK) {
-        rc = st == kLoading ? load(*r) : solve(*r, wctx);
+        rc = loading ? load(*batch[0]) : solve(batch, wctx);
         if (rc != RR_OK) err = rr_last_error();
       }
       std::lock_guard<std::mutex> lk(mu);
-      if (rc != RR_OK) {
-        r->error = err;
-        release(*r);
-        finish_locked(*r, rc);
-      } else if (st == kLoading) {
-        r->state = kRunning;
-        running.push_back(id);
-        cv_sched.notify_one();
-      } else {
-        release(*r);
-        finish_locked(*r, RR_OK);
+      for (Request* r : batch) {
+        if (rc != RR_OK) {
+          r->error = err;
+          release(*r);
+          finish_locked(*r, rc);
+        } else if (loading) {
+          r->state = kRunning;
+          running.push_back(r->id);
+          cv_sched.notify_one();
+        } else {
+          release(*r);
+          finish_locked(*r, RR_OK);
+        }
       }
     }
     if (wctx) rr_ctx_destroy(wctx);
@@ -297,7 +332,7 @@ struct rr_server_s {
         for (uint64_t id : finished) {
           running.erase(std::find(running.begin(), running.end(), id));
           reqs[id]->state = kSolving;
-          tasks.push_back(id);
+          solve_q.push_back(id);
           cv_work.notify_one();
         }
         for (size_t q = 0; q < failed.size(); ++q) {
