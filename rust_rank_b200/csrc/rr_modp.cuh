@@ -19,9 +19,18 @@ struct ModP {
 };
 
 #ifdef __CUDACC__
+// a * b + c exactly (mod 2^64), as a carry chain of 32-bit multiply-adds
+// (mad.lo.cc / madc.hi): on sm_100 this issues at about 1.6x the rate of the
+// 64-bit wide multiply-add the compiler emits for (uint64_t)a * b + c.
+__device__ __forceinline__ uint64_t mad_wide(uint32_t a, uint32_t b, uint64_t c) {
+  uint32_t lo = (uint32_t)c, hi = (uint32_t)(c >> 32);
+  asm("mad.lo.cc.u32 %0, %2, %3, %0;\n\tmadc.hi.u32 %1, %2, %3, %1;" : "+r"(lo), "+r"(hi) : "r"(a), "r"(b));
+  return ((uint64_t)hi << 32) | lo;
+}
+
 // Fold a 64-bit accumulator: result == x (mod p) and result < 2^32 * c32 + 2^32.
 __device__ __forceinline__ uint64_t fold(uint64_t x, const ModP& M) {
-  return (uint64_t)(uint32_t)(x >> 32) * M.c32 + (uint32_t)x;
+  return mad_wide((uint32_t)(x >> 32), M.c32, (uint32_t)x);
 }
 
 // Exact x mod p for any 64-bit x.  q = floor(x*mu / 2^64) is at most 2 below
@@ -56,10 +65,6 @@ __device__ __forceinline__ uint32_t addmod(uint32_t a, uint32_t b, uint32_t p) {
 
 __device__ __forceinline__ uint32_t submod(uint32_t a, uint32_t b, uint32_t p) {
   return a >= b ? a - b : a + p - b;
-}
-
-__device__ __forceinline__ uint64_t mad_wide(uint32_t a, uint32_t b, uint64_t c) {
-  return (uint64_t)a * b + c;
 }
 
 // (hi:lo) += a * b with a carry chain of 32-bit multiply-adds; on sm_100 this
