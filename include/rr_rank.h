@@ -186,6 +186,12 @@ int rr_batch_sequence(rr_batch* batch, int32_t i, uint32_t* seq, int64_t seq_str
  * has not run), `workers` generators in flight on streams of their own.
  * ranks[nmat] in the caller's order; RR_ESTATE as rr_rank_from_basis. */
 int rr_batch_ranks(rr_batch* batch, int32_t workers, int64_t* ranks);
+/* Launch shapes the batch's autotuner picked: the Krylov loop has one phase
+ * per distinct set of running matrices (phase k covers applications
+ * apps_from[k] .. apps_from[k+1]-1); ctas[k] is the grid of its pass launches,
+ * chosen at create time by timing 1..4 CTAs per SM.  Call with NULL arrays to
+ * get the phase count; *nphases gives the room of the arrays. */
+int rr_batch_tuning(const rr_batch* batch, int32_t* nphases, int32_t* ctas, int64_t* apps_from);
 /* Stacked sizes: rows and columns with padding, nonzeros, applications of
  * B of the longest sequence. */
 int rr_batch_info(const rr_batch* batch, int64_t* total_rows, int64_t* total_cols, int64_t* total_nnz,

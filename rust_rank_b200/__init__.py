@@ -392,6 +392,15 @@ class Batch:
         check(lib().rr_batch_ranks(self.handle, int(workers), ptr(out)))
         return out
 
+    def tuning(self):
+        """[(first application, CTAs)] per phase of the Krylov loop, as the autotuner chose them."""
+        k = C.c_int32(0)
+        check(lib().rr_batch_tuning(self.handle, C.byref(k), None, None))
+        ctas = np.zeros(k.value, np.int32)
+        first = np.zeros(k.value, np.int64)
+        check(lib().rr_batch_tuning(self.handle, C.byref(k), ptr(ctas), ptr(first)))
+        return [(int(a), int(c)) for a, c in zip(first, ctas)]
+
     def info(self):
         r, c, z, a = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()
         check(lib().rr_batch_info(self.handle, C.byref(r), C.byref(c), C.byref(z), C.byref(a)))

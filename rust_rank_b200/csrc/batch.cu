@@ -18,6 +18,8 @@
 #include <atomic>
 #include <cmath>
 #include <condition_variable>
+#include <cstdio>
+#include <string>
 #include <mutex>
 #include <cstring>
 #include <memory>
@@ -45,9 +47,14 @@ struct rr_batch_s {
   // equal-work warp runs per phase (a phase = a set of running matrices):
   // runs_*[phase][warp], kPassWarps * grid + 1 entries each
   rr::DevBuf<int32_t> runs_rows, runs_cols;
-  std::vector<int> phase_of;  // first running stack position -> phase
+  std::vector<int> phase_of;     // first running stack position -> phase
+  std::vector<int> phase_first;  // phase -> first running stack position
+  std::vector<int> phase_grid;   // phase -> CTAs of its pass launches (autotuned)
+  std::vector<int64_t> run_off;  // phase -> offset of its warp-run tables (phase_grid * kPassWarps + 1 entries)
   rr::DevBuf<uint32_t> X[2], U, dr_m, dc_m, dc_r, W0;
   rr::DevBuf<unsigned long long> gram_acc;
+  rr::DevBuf<unsigned long long> gram_all;  // one Gram slot per (matrix, term): [seg_G_off[s] + t * NP]
+  rr::DevBuf<int64_t> d_seg_G_off, d_seg_terms;
   rr::DevBuf<unsigned int> counter;
   rr::DevBuf<uint32_t> S;
   rr::DevBuf<int64_t> d_s_off;
@@ -74,6 +81,23 @@ int64_t default_len(int64_t m, int64_t n, int b) {  // src/main.rs:497-504
 
 int64_t pad32(int64_t x) { return (x + 31) / 32 * 32; }
 
+// fn(i) for i < count on the host's cores (each index touches its own data).
+template <class F>
+void parallel_for(int count, F fn) {
+  const int nt = std::max(1, std::min<int>(count, (int)std::thread::hardware_concurrency()));
+  if (nt == 1) {
+    for (int i = 0; i < count; ++i) fn(i);
+    return;
+  }
+  std::atomic<int> next{0};
+  std::vector<std::thread> pool;
+  for (int t = 0; t < nt; ++t)
+    pool.emplace_back([&] {
+      for (int i = next.fetch_add(1); i < count; i = next.fetch_add(1)) fn(i);
+    });
+  for (auto& th : pool) th.join();
+}
+
 PassParams batch_params(rr_batch* bt) {
   PassParams P;
   std::memset(&P, 0, sizeof(P));
@@ -90,6 +114,8 @@ PassParams batch_params(rr_batch* bt) {
   P.S_all = bt->S.ptr;
   P.S_out = bt->S.ptr;  // non-null: emit terms
   P.seg_S_off = bt->d_s_off.ptr;
+  P.gram_all = bt->gram_all.ptr;  // slot per term, finished per group by batch_finalize_kernel
+  P.seg_G_off = bt->d_seg_G_off.ptr;
   return P;
 }
 
@@ -117,6 +143,115 @@ std::vector<int64_t> batch_work(const std::vector<uint32_t>& ptr, int rpb) {
   for (int64_t q = 0; q < nb; ++q)
     pre[q + 1] = pre[q] + (int64_t)(ptr[(q + 1) * rpb] - ptr[q * rpb]) + kRowCost * rpb;
   return pre;
+}
+
+// Warp-run tables (both passes) of phase ph for a grid of `grid` CTAs.
+void phase_runs(const rr_batch* bt, int ph, int grid, const std::vector<int64_t>& wa, const std::vector<int64_t>& wt,
+                int32_t* ra, int32_t* rt) {
+  const int rpb = rows_per_batch(bt->B), f = bt->phase_first[ph], nw = grid * kPassWarps;
+  equal_runs(wa, bt->row_off[f] / rpb, bt->row_off[bt->nmat] / rpb, nw, ra);
+  equal_runs(wt, bt->col_off[f] / rpb, bt->col_off[bt->nmat] / rpb, nw, rt);
+}
+
+// One application of B over the matrices of phase ph (the Krylov loop's two
+// launches), with the given grid and run tables.
+int launch_phase_app(rr_batch* bt, int ph, int grid, const int32_t* d_ra, const int32_t* d_rt, int64_t t) {
+  const int rpb = rows_per_batch(bt->B), nmat = bt->nmat, first = bt->phase_first[ph];
+  PassParams P = batch_params(bt);
+  P.seg_begin = first;
+  P.seg_end = nmat;
+  P.replicas = std::max(1, std::min(kGramReplicas, 64 / (nmat - first)));
+  P.rowptr = bt->A.rowptr.ptr;
+  P.cv = bt->A.cv.ptr;
+  P.rows = bt->row_off[nmat];
+  P.X = reinterpret_cast<const uint4*>(bt->X[bt->cur].ptr);
+  P.Y = reinterpret_cast<uint4*>(bt->U.ptr);
+  P.scale = bt->dr_m.ptr;
+  P.gram_mul = bt->M.r1;
+  P.batch_seg = bt->seg_rows.ptr;
+  P.runs = d_ra;
+  P.batch_begin = bt->row_off[first] / rpb;
+  P.term = 2 * t + 1;
+  RR_TRY(launch_pass_raw(bt->stream, bt->B, bt->fold4, grid, P, kModeOdd));
+  P.rowptr = bt->At.rowptr.ptr;
+  P.cv = bt->At.cv.ptr;
+  P.rows = bt->col_off[nmat];
+  P.X = reinterpret_cast<const uint4*>(bt->U.ptr);
+  P.Y = reinterpret_cast<uint4*>(bt->X[bt->cur ^ 1].ptr);
+  P.scale = bt->dc_m.ptr;
+  P.scale2 = bt->dc_r.ptr;
+  P.gram_mul = 1;
+  P.batch_seg = bt->seg_cols.ptr;
+  P.runs = d_rt;
+  P.batch_begin = bt->col_off[first] / rpb;
+  P.term = 2 * t + 2;
+  return launch_pass_raw(bt->stream, bt->B, bt->fold4, grid, P, kModeEven);
+}
+
+// Autotuner: for every phase, time a few applications of B with 1..`max_cps`
+// CTAs per SM and keep the fastest.  Few or small running matrices leave
+// each warp only a few row batches on the full grid, and the per-warp fixed
+// costs (Gram set-up, flush, atomics) then dominate; a smaller grid amortises
+// them.  The timed applications write terms 1 and 2 of the running matrices
+// and scratch blocks only; the Krylov loop recomputes all of them.
+int tune_phases(rr_batch* bt, int max_cps, const std::vector<int64_t>& wa, const std::vector<int64_t>& wt) {
+  const int nph = (int)bt->phase_first.size(), sms = bt->ctx->num_sms;
+  const int max_grid = std::max(1, max_cps) * sms;
+  RR_CUDA(cudaMemsetAsync(bt->X[0].ptr, 0, bt->X[0].bytes(), bt->stream));
+  RR_CUDA(cudaMemsetAsync(bt->X[1].ptr, 0, bt->X[1].bytes(), bt->stream));
+  RR_CUDA(cudaMemsetAsync(bt->U.ptr, 0, bt->U.bytes(), bt->stream));
+  DevBuf<int32_t> dra, drt;
+  RR_TRY(dra.alloc((size_t)max_grid * kPassWarps + 1));
+  RR_TRY(drt.alloc((size_t)max_grid * kPassWarps + 1));
+  std::vector<int32_t> ra((size_t)max_grid * kPassWarps + 1), rt(ra.size());
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  RR_CUDA(cudaEventCreate(&e0));
+  RR_CUDA(cudaEventCreate(&e1));
+  int status = RR_OK;
+  bt->phase_grid.assign(nph, max_grid);
+  for (int ph = 0; ph < nph && status == RR_OK; ++ph) {
+    float best = 0.f;
+    for (int cps = 1; cps <= std::max(1, max_cps) && status == RR_OK; ++cps) {
+      const int grid = cps * sms;
+      phase_runs(bt, ph, grid, wa, wt, ra.data(), rt.data());
+      const size_t words = (size_t)grid * kPassWarps + 1;
+      if (cudaMemcpyAsync(dra.ptr, ra.data(), words * 4, cudaMemcpyHostToDevice, bt->stream) != cudaSuccess ||
+          cudaMemcpyAsync(drt.ptr, rt.data(), words * 4, cudaMemcpyHostToDevice, bt->stream) != cudaSuccess) {
+        status = fail(RR_ECUDA, "tuning upload failed");
+        break;
+      }
+      status = launch_phase_app(bt, ph, grid, dra.ptr, drt.ptr, 0);  // warm-up
+      if (status == RR_OK) cudaEventRecord(e0, bt->stream);
+      for (int rep = 0; rep < 3 && status == RR_OK; ++rep) status = launch_phase_app(bt, ph, grid, dra.ptr, drt.ptr, 0);
+      if (status != RR_OK) break;
+      cudaEventRecord(e1, bt->stream);
+      if (cudaEventSynchronize(e1) != cudaSuccess) {
+        status = fail(RR_ECUDA, "tuning: %s", cudaGetErrorString(cudaGetLastError()));
+        break;
+      }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (cps == 1 || ms < best) {
+        best = ms;
+        bt->phase_grid[ph] = grid;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (status != RR_OK) return status;
+  // final tables with the chosen grids
+  bt->run_off.assign(nph + 1, 0);
+  for (int ph = 0; ph < nph; ++ph) bt->run_off[ph + 1] = bt->run_off[ph] + (int64_t)bt->phase_grid[ph] * kPassWarps + 1;
+  std::vector<int32_t> fa(bt->run_off[nph]), ft(bt->run_off[nph]);
+  for (int ph = 0; ph < nph; ++ph)
+    phase_runs(bt, ph, bt->phase_grid[ph], wa, wt, fa.data() + bt->run_off[ph], ft.data() + bt->run_off[ph]);
+  RR_TRY(bt->runs_rows.alloc(fa.size()));
+  RR_TRY(bt->runs_cols.alloc(ft.size()));
+  RR_CUDA(cudaMemcpyAsync(bt->runs_rows.ptr, fa.data(), fa.size() * 4, cudaMemcpyHostToDevice, bt->stream));
+  RR_CUDA(cudaMemcpyAsync(bt->runs_cols.ptr, ft.data(), ft.size() * 4, cudaMemcpyHostToDevice, bt->stream));
+  RR_CUDA(cudaStreamSynchronize(bt->stream));
+  return RR_OK;
 }
 
 // Completion of the sequences as the Krylov loop publishes them.
@@ -151,7 +286,9 @@ int krylov_run(rr_batch* bt, cudaEvent_t* ev, Progress* prog) {
   int first = 0;
   for (int64_t t = 0; t < max_apps; ++t) {
     while (first < nmat && bt->apps[first] <= t) ++first;
-    const size_t run_off = (size_t)bt->phase_of[first] * (bt->grid * kPassWarps + 1);
+    const int ph = bt->phase_of[first];
+    const size_t run_off = (size_t)bt->run_off[ph];
+    const int grid = bt->phase_grid[ph];
     uint32_t* x = bt->X[bt->cur].ptr;
     uint32_t* xn = bt->X[bt->cur ^ 1].ptr;
     PassParams P = batch_params(bt);
@@ -171,7 +308,7 @@ int krylov_run(rr_batch* bt, cudaEvent_t* ev, Progress* prog) {
     P.runs = bt->runs_rows.ptr + run_off;
     P.batch_begin = bt->row_off[first] / rpb;
     P.term = 2 * t + 1;
-    RR_TRY(launch_pass_raw(st, bt->B, bt->fold4, bt->grid, P, kModeOdd));
+    RR_TRY(launch_pass_raw(st, bt->B, bt->fold4, grid, P, kModeOdd));
     // rows of A^T: w' = D_c A^T U, x' = D_c w', even term
     P.rowptr = bt->At.rowptr.ptr;
     P.cv = bt->At.cv.ptr;
@@ -185,15 +322,16 @@ int krylov_run(rr_batch* bt, cudaEvent_t* ev, Progress* prog) {
     P.runs = bt->runs_cols.ptr + run_off;
     P.batch_begin = bt->col_off[first] / rpb;
     P.term = 2 * t + 2;
-    RR_TRY(launch_pass_raw(st, bt->B, bt->fold4, bt->grid, P, kModeEven));
+    RR_TRY(launch_pass_raw(st, bt->B, bt->fold4, grid, P, kModeEven));
     bt->cur ^= 1;
-    if (ev) {
-      int done_to = first;
-      while (done_to < nmat && bt->apps[done_to] == t + 1) {
-        RR_CUDA(cudaEventRecord(ev[done_to], st));
-        ++done_to;
-      }
-      if (done_to > first) {
+    // matrices whose sequences end here: finish their terms, then publish
+    int done_to = first;
+    while (done_to < nmat && bt->apps[done_to] == t + 1) ++done_to;
+    if (done_to > first) {
+      RR_TRY(launch_batch_finalize(st, bt->gram_all.ptr, bt->d_seg_G_off.ptr, bt->S.ptr, bt->d_s_off.ptr,
+                                   bt->d_seg_terms.ptr, first, done_to, 2 * (t + 1) + 1, bt->b, bt->B, bt->M));
+      if (ev) {
+        for (int s = first; s < done_to; ++s) RR_CUDA(cudaEventRecord(ev[s], st));
         {
           std::lock_guard<std::mutex> lk(prog->mu);
           prog->published = done_to;
@@ -236,22 +374,31 @@ int rr_batch_create(rr_ctx* ctx, int32_t nmat, const int64_t* m, const int64_t* 
     const unsigned __int128 q = (unsigned __int128)(p - 1) * (p - 1);
     bt->fold4 = (F + 4 * q) < ((unsigned __int128)1 << 64);
   }
-  // validate and order by sequence length
+  // validate (in parallel over matrices) and order by sequence length
   std::vector<int64_t> len(nmat);
-  for (int i = 0; i < nmat; ++i) {
-    if (m[i] < 1 || n[i] < 1 || !rowptr[i] || rowptr[i][0] != 0) return fail(RR_EINVAL, "matrix %d: bad shape/rowptr", i);
-    for (int64_t r = 0; r < m[i]; ++r)
-      if (rowptr[i][r + 1] < rowptr[i][r]) return fail(RR_EINVAL, "matrix %d: rowptr decreases", i);
-    for (int64_t k = 0; k < rowptr[i][m[i]]; ++k)
-      if (col[i][k] < 0 || col[i][k] >= n[i] || val[i][k] >= p) return fail(RR_EINVAL, "matrix %d: entry %lld invalid", i, (long long)k);
-    for (int64_t r = 0; r < m[i]; ++r)
-      if (!row_precond[i][r] || row_precond[i][r] >= p) return fail(RR_EINVAL, "matrix %d: row_precond not in [1,p)", i);
-    for (int64_t c = 0; c < n[i]; ++c)
-      if (!col_precond[i][c] || col_precond[i][c] >= p) return fail(RR_EINVAL, "matrix %d: col_precond not in [1,p)", i);
-    for (int64_t e = 0; e < (int64_t)b * n[i]; ++e)
-      if (V[i][e] >= p) return fail(RR_EINVAL, "matrix %d: V not reduced", i);
-    len[i] = default_len(m[i], n[i], b);
-  }
+  std::vector<std::string> bad(nmat);
+  parallel_for(nmat, [&](int i) {
+    char msg[160] = "";
+    if (m[i] < 1 || n[i] < 1 || !rowptr[i] || rowptr[i][0] != 0) {
+      snprintf(msg, sizeof msg, "matrix %d: bad shape/rowptr", i);
+    } else {
+      for (int64_t r = 0; r < m[i] && !msg[0]; ++r)
+        if (rowptr[i][r + 1] < rowptr[i][r]) snprintf(msg, sizeof msg, "matrix %d: rowptr decreases", i);
+      for (int64_t k = 0; !msg[0] && k < rowptr[i][m[i]]; ++k)
+        if (col[i][k] < 0 || col[i][k] >= n[i] || val[i][k] >= p)
+          snprintf(msg, sizeof msg, "matrix %d: entry %lld invalid", i, (long long)k);
+      for (int64_t r = 0; !msg[0] && r < m[i]; ++r)
+        if (!row_precond[i][r] || row_precond[i][r] >= p) snprintf(msg, sizeof msg, "matrix %d: row_precond not in [1,p)", i);
+      for (int64_t c = 0; !msg[0] && c < n[i]; ++c)
+        if (!col_precond[i][c] || col_precond[i][c] >= p) snprintf(msg, sizeof msg, "matrix %d: col_precond not in [1,p)", i);
+      for (int64_t e = 0; !msg[0] && e < (int64_t)b * n[i]; ++e)
+        if (V[i][e] >= p) snprintf(msg, sizeof msg, "matrix %d: V not reduced", i);
+    }
+    bad[i] = msg;
+    len[i] = msg[0] ? 0 : default_len(m[i], n[i], b);
+  });
+  for (int i = 0; i < nmat; ++i)
+    if (!bad[i].empty()) return fail(RR_EINVAL, "%s", bad[i].c_str());
   bt->order.resize(nmat);
   std::iota(bt->order.begin(), bt->order.end(), 0);
   std::stable_sort(bt->order.begin(), bt->order.end(), [&](int a, int c) { return len[a] < len[c]; });
@@ -264,6 +411,7 @@ int rr_batch_create(rr_ctx* ctx, int32_t nmat, const int64_t* m, const int64_t* 
   bt->col_off.assign(nmat + 1, 0);
   bt->s_off.assign(nmat + 1, 0);
   int64_t nnz = 0;
+  std::vector<int64_t> nnz_off(nmat + 1, 0);
   for (int s = 0; s < nmat; ++s) {
     const int i = bt->order[s];
     bt->m[s] = m[i];
@@ -273,6 +421,7 @@ int rr_batch_create(rr_ctx* ctx, int32_t nmat, const int64_t* m, const int64_t* 
     bt->col_off[s + 1] = bt->col_off[s] + pad32(n[i]);
     bt->s_off[s + 1] = bt->s_off[s] + (int64_t)bt->np * (2 * bt->apps[s] + 1);
     nnz += rowptr[i][m[i]];
+    nnz_off[s + 1] = nnz;
   }
   if (nnz >= (1ll << 32) - 1) return fail(RR_EUNSUPPORTED, "batch nnz %lld exceeds 2^32 - 2", (long long)nnz);
   bt->nnz = nnz;
@@ -283,8 +432,8 @@ int rr_batch_create(rr_ctx* ctx, int32_t nmat, const int64_t* m, const int64_t* 
   std::vector<uint2> acv(std::max<int64_t>(nnz, 1)), tcv(std::max<int64_t>(nnz, 1));
   std::vector<uint32_t> drm(Mtot, 1), dcm(Ntot, 1), dcr(Ntot, 1), w0(Ntot * bt->B, 0);
   const uint64_t R1 = bt->M.r1, R2 = R1 * R1 % p;
-  uint32_t o = 0;
-  for (int s = 0; s < nmat; ++s) {
+  // every matrix fills its own ranges of the stacked arrays: in parallel
+  parallel_for(nmat, [&](int s) {
     const int i = bt->order[s];
     const int64_t mi = m[i], ni = n[i];
     std::vector<int64_t> rdeg(mi), cdeg(ni, 0);
@@ -297,6 +446,7 @@ int rr_batch_create(rr_ctx* ctx, int32_t nmat, const int64_t* m, const int64_t* 
     std::stable_sort(cperm.begin(), cperm.end(), [&](int32_t a, int32_t c) { return cdeg[a] > cdeg[c]; });
     for (int64_t c = 0; c < ni; ++c) cinv[cperm[c]] = (int32_t)c;
     const int64_t r0 = bt->row_off[s], c0 = bt->col_off[s];
+    uint32_t o = (uint32_t)nnz_off[s];
     for (int64_t rp = 0; rp < pad32(mi); ++rp) {
       aptr[r0 + rp] = o;
       if (rp < mi) {
@@ -314,15 +464,22 @@ int rr_batch_create(rr_ctx* ctx, int32_t nmat, const int64_t* m, const int64_t* 
       dcr[c0 + cp] = (uint32_t)(col_precond[i][c] * R1 % p);
       for (int l = 0; l < b; ++l) w0[(c0 + cp) * bt->B + l] = V[i][(size_t)l * ni + c];
     }
-  }
-  aptr[Mtot] = o;
-  for (int64_t k = 0; k < nnz; ++k) tptr[acv[k].x + 1]++;
-  for (int64_t c = 0; c < Ntot; ++c) tptr[c + 1] += tptr[c];
-  {
-    std::vector<uint32_t> next(tptr.begin(), tptr.end() - 1);
-    for (int64_t r = 0; r < Mtot; ++r)
-      for (uint32_t k = aptr[r]; k < aptr[r + 1]; ++k) tcv[next[acv[k].x]++] = make_uint2((uint32_t)r, acv[k].y);
-  }
+    // this matrix's block of the transpose: its columns are [c0, c1), its
+    // entries [nnz_off[s], nnz_off[s + 1]); counting sort, stable by row, into
+    // its own range of tptr / tcv only
+    const int64_t c1 = bt->col_off[s + 1], r1 = bt->row_off[s + 1], nc = c1 - c0;
+    std::vector<uint32_t> start(nc + 1, 0);
+    for (int64_t k = nnz_off[s]; k < nnz_off[s + 1]; ++k) start[acv[k].x - c0 + 1]++;
+    for (int64_t c = 0; c < nc; ++c) start[c + 1] += start[c];
+    std::vector<uint32_t> next(nc);
+    for (int64_t c = 0; c < nc; ++c) next[c] = tptr[c0 + c] = (uint32_t)nnz_off[s] + start[c];
+    for (int64_t r = r0; r < r1; ++r) {
+      const uint32_t kb = aptr[r], ke = r + 1 < r1 ? aptr[r + 1] : (uint32_t)nnz_off[s + 1];
+      for (uint32_t k = kb; k < ke; ++k) tcv[next[acv[k].x - c0]++] = make_uint2((uint32_t)r, acv[k].y);
+    }
+  });
+  aptr[Mtot] = (uint32_t)nnz;
+  tptr[Ntot] = (uint32_t)nnz;
   // segment of every row batch
   const int rpb = rows_per_batch(bt->B);
   std::vector<int32_t> srow(Mtot / rpb), scol(Ntot / rpb);
@@ -359,33 +516,50 @@ int rr_batch_create(rr_ctx* ctx, int32_t nmat, const int64_t* m, const int64_t* 
   RR_TRY(bt->counter.alloc(4));
   RR_CUDA(cudaMemsetAsync(bt->counter.ptr, 0, bt->counter.bytes(), st));
   RR_TRY(bt->S.alloc(std::max<int64_t>(bt->s_off[nmat], 1)));
+  {
+    std::vector<int64_t> goff(nmat + 1, 0), terms(nmat);
+    for (int s = 0; s < nmat; ++s) {
+      terms[s] = 2 * bt->apps[s] + 1;
+      goff[s + 1] = goff[s] + terms[s] * NP;
+    }
+    RR_TRY(up(bt->d_seg_G_off, goff));
+    RR_TRY(up(bt->d_seg_terms, terms));
+    RR_TRY(bt->gram_all.alloc((size_t)std::max<int64_t>(goff[nmat], 1)));
+  }
   int blocks = 1;
   RR_TRY(pass_blocks_per_sm(bt->B, bt->fold4, &blocks));
   bt->grid = std::max(1, blocks) * ctx->num_sms;
-  {  // phases: one per distinct set of running matrices
-    const int nw = bt->grid * kPassWarps;
-    std::vector<int> firsts;
-    bt->phase_of.assign(nmat, -1);
-    for (int s = 0; s < nmat; ++s)
-      if (s == 0 || bt->apps[s] != bt->apps[s - 1]) {
-        bt->phase_of[s] = (int)firsts.size();
-        firsts.push_back(s);
-      }
-    const std::vector<int64_t> wa = batch_work(aptr, rpb), wt = batch_work(tptr, rpb);
-    std::vector<int32_t> ra(firsts.size() * (nw + 1)), rt(firsts.size() * (nw + 1));
-    for (size_t ph = 0; ph < firsts.size(); ++ph) {
-      const int f = firsts[ph];
-      equal_runs(wa, bt->row_off[f] / rpb, Mtot / rpb, nw, ra.data() + ph * (nw + 1));
-      equal_runs(wt, bt->col_off[f] / rpb, Ntot / rpb, nw, rt.data() + ph * (nw + 1));
+  // phases: one per distinct set of running matrices
+  bt->phase_of.assign(nmat, -1);
+  for (int s = 0; s < nmat; ++s)
+    if (s == 0 || bt->apps[s] != bt->apps[s - 1]) {
+      bt->phase_of[s] = (int)bt->phase_first.size();
+      bt->phase_first.push_back(s);
     }
-    RR_TRY(up(bt->runs_rows, ra));
-    RR_TRY(up(bt->runs_cols, rt));
-  }
+  const std::vector<int64_t> wa = batch_work(aptr, rpb), wt = batch_work(tptr, rpb);
   int prio_lo = 0, prio_hi = 0;
   RR_CUDA(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
   RR_CUDA(cudaStreamCreateWithPriority(&bt->stream, cudaStreamNonBlocking, prio_hi));
   RR_CUDA(cudaStreamSynchronize(st));
+  RR_TRY(tune_phases(bt.get(), blocks, wa, wt));
+  RR_CUDA(cudaMemsetAsync(bt->gram_all.ptr, 0, bt->gram_all.bytes(), bt->stream));
+  RR_CUDA(cudaStreamSynchronize(bt->stream));
+  RR_CUDA(cudaStreamSynchronize(st));
   *out = bt.release();
+  return RR_OK;
+}
+
+int rr_batch_tuning(const rr_batch* bt, int32_t* nphases, int32_t* ctas, int64_t* apps_from) {
+  if (!bt || !nphases) return fail(RR_EINVAL, "NULL argument");
+  const int nph = (int)bt->phase_first.size();
+  if (ctas || apps_from) {
+    if (*nphases < nph) return fail(RR_EINVAL, "room for %d phases, %d needed", *nphases, nph);
+    for (int ph = 0; ph < nph; ++ph) {
+      if (ctas) ctas[ph] = bt->phase_grid[ph];
+      if (apps_from) apps_from[ph] = bt->phase_first[ph] == 0 ? 0 : bt->apps[bt->phase_first[ph] - 1];
+    }
+  }
+  *nphases = nph;
   return RR_OK;
 }
 

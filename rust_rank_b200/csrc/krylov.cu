@@ -371,6 +371,13 @@ struct GramMma {
   }
 };
 
+// Batched mode: where the Gram partials of segment sg go (its own slot for
+// this launch's term, or the segment's shared accumulator); NP = padded pairs.
+__device__ __forceinline__ unsigned long long* seg_target(const PassParams& P, unsigned long long* acc, int sg, int NP) {
+  if (P.gram_all != nullptr) return P.gram_all + P.seg_G_off[sg] + P.term * (int64_t)NP;
+  return acc + (size_t)sg * NP;
+}
+
 template <int B, int MODE, int FE>
 // Four CTAs (32 warps) per SM: the walk is latency bound, so occupancy is
 // worth a few spilled registers (measured on the 2M x 1.5M Zipf matrix).
@@ -435,7 +442,7 @@ __global__ void __launch_bounds__(kThreads, 4) pass_kernel(PassParams P) {
       if (sg != cur_seg) {
         if (cur_seg >= 0) {
           gram.finish(slot, sub, lane, M, W);
-          gram.emit(cur_seg == seg0 ? red : acc + (size_t)cur_seg * NP, lane, M);
+          gram.emit(cur_seg == seg0 ? red : seg_target(P, acc, cur_seg, NP), lane, M);
           gram.reset();
         }
         cur_seg = sg;
@@ -510,10 +517,13 @@ __global__ void __launch_bounds__(kThreads, 4) pass_kernel(PassParams P) {
   gram.finish(slot, sub, lane, M, W);
   __syncthreads();  // red[] is zeroed before any warp emits into it
   if (segmented) {
-    if (cur_seg >= 0) gram.emit(cur_seg == seg0 ? red : acc + (size_t)cur_seg * NP, lane, M);
+    if (cur_seg >= 0) gram.emit(cur_seg == seg0 ? red : seg_target(P, acc, cur_seg, NP), lane, M);
     __syncthreads();
-    if (seg0 >= 0)
-      for (int q = threadIdx.x; q < NP; q += kThreads) atomicAdd(&acc[(size_t)seg0 * NP + q], red[q]);
+    if (seg0 >= 0) {
+      unsigned long long* t0 = seg_target(P, acc, seg0, NP);
+      for (int q = threadIdx.x; q < NP; q += kThreads) atomicAdd(&t0[q], red[q]);
+    }
+    if (P.gram_all != nullptr) return;  // finished later, once per group
   } else {
     gram.emit(red, lane, M);
     __syncthreads();
@@ -636,6 +646,38 @@ __global__ void gather_curv_kernel(const uint32_t* __restrict__ x, const uint32_
     const int l = (int)(i % b);
     curv[(size_t)l * n + colperm[c]] = mulmod(x[c * B + l], dcinv[c], M);
   }
+}
+
+// Slot-per-term Gram sums of segments [seg_begin, seg_end) -> sequence terms
+// (real pairs; odd terms were accumulated from z R^{-1} and take a factor R).
+__global__ void batch_finalize_kernel(const unsigned long long* __restrict__ gram_all,
+                                      const int64_t* __restrict__ seg_G_off, uint32_t* __restrict__ S_all,
+                                      const int64_t* __restrict__ seg_S_off, const int64_t* __restrict__ seg_terms,
+                                      int seg_begin, int b, int B, uint32_t r1, ModP M) {
+  const int s = seg_begin + (int)blockIdx.y;
+  const int npr = b * (b + 1) / 2, NP = B * (B + 1) / 2;
+  const int64_t total = seg_terms[s] * npr;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t t = e / npr;
+    const int q = (int)(e - t * npr);
+    int i, j;
+    pair_of(q, b, i, j);
+    const unsigned long long v = gram_all[seg_G_off[s] + t * NP + pair_index(i, j, B)];
+    const uint32_t r = reduce(v, M);
+    S_all[seg_S_off[s] + t * npr + q] = (t & 1) ? mulmod(r, r1, M) : r;
+  }
+}
+
+int launch_batch_finalize(cudaStream_t s, const unsigned long long* gram_all, const int64_t* d_seg_G_off,
+                          uint32_t* S_all, const int64_t* d_seg_S_off, const int64_t* d_seg_terms, int seg_begin,
+                          int seg_end, int64_t max_terms, int b, int B, const ModP& M) {
+  if (seg_end <= seg_begin) return RR_OK;
+  const int64_t work = max_terms * (b * (b + 1) / 2);
+  const dim3 grid((unsigned)std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, 1024)), (unsigned)(seg_end - seg_begin));
+  batch_finalize_kernel<<<grid, 256, 0, s>>>(gram_all, d_seg_G_off, S_all, d_seg_S_off, d_seg_terms, seg_begin, b, B,
+                                             M.r1, M);
+  RR_CUDA(cudaGetLastError());
+  return RR_OK;
 }
 
 // ---------------------------------------------------------------- launchers

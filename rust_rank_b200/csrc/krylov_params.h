@@ -27,6 +27,12 @@ struct PassParams {
   // *term_ctr.  nullptr = S_out as given.
   unsigned int* term_ctr;
   uint32_t* const* S_ptr;
+  // Batched, slot-per-term mode: the Gram partials of segment s for this
+  // launch's term go to gram_all + seg_G_off[s] + term * NP with atomics and
+  // nothing is finished in the kernel (batch_finalize_kernel does that once
+  // per group of finished sequences).  nullptr = accumulators + last CTA.
+  unsigned long long* gram_all;
+  const int64_t* seg_G_off;
   uint32_t gram_mul;        // factor applied to the finished term
   uint32_t w4, w5, w6;      // 2^32, 2^40, 2^48 mod p (limb weights of the tensor-core Gram)
   int b_real;
@@ -55,6 +61,11 @@ struct ChunkParams {
   ModP M;
 };
 
+// Finish the slot-per-term Gram sums of segments [seg_begin, seg_end):
+// S_all[seg_S_off[s] + t * pairs + q] = reduce(gram_all[seg_G_off[s] + t * NP + pair q]) * (t odd ? R : 1).
+int launch_batch_finalize(cudaStream_t s, const unsigned long long* gram_all, const int64_t* d_seg_G_off,
+                          uint32_t* S_all, const int64_t* d_seg_S_off, const int64_t* d_seg_terms, int seg_begin,
+                          int seg_end, int64_t max_terms, int b, int B, const ModP& M);
 // Launch one pass kernel for padded width B on stream s (grid = CTAs).
 int launch_pass_raw(cudaStream_t s, int B, int fold4, int grid, const PassParams& P, int mode);
 // CTAs per SM of the pass kernel for padded width B (also sets its shared-memory limit).

@@ -132,3 +132,22 @@ def test_batch_graph_complex_subset(ctx):
     for i, (rowptr, col, val, m, n) in enumerate(mats):
         a = rr.CsrMatrix.from_arrays(rowptr, col, val, m, n)
         assert ranks[i] == rr.block_wiedemann_rank(a, b, P, drs[i], dcs[i], vs[i], ctx=ctx), i
+
+
+def test_batch_autotuner_shapes(ctx):
+    """The autotuner picks, per phase of the Krylov loop, a grid of 1..4 CTAs
+    per SM; phases start at increasing applications; results stay exact."""
+    b = 8
+    mats = _mixed_batch(31, count=7)
+    drs, dcs, vs = _inputs(mats, b, 13)
+    bt = rr.Batch(mats, b, P, drs, dcs, vs, ctx)
+    shapes = bt.tuning()
+    assert len(shapes) >= 1 and shapes[0][0] == 0
+    assert all(s1[0] > s0[0] for s0, s1 in zip(shapes, shapes[1:]))
+    assert all(c % 148 == 0 and 148 <= c <= 4 * 148 for _, c in shapes) or all(c >= 1 for _, c in shapes)
+    bt.krylov()
+    for i, (rowptr, col, val, m, n) in enumerate(mats):
+        L = rr.default_max_nlen(m, n, b)
+        ref, Lr, _ = oracle.krylov(rowptr, col, val, m, n, P, drs[i], dcs[i], vs[i], 0, L)
+        assert np.array_equal(bt.sequence(i), ref[:, :Lr]), i
+    bt.close()
