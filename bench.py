@@ -246,7 +246,7 @@ def rank_pipeline(ctx, reps=3):
             "timing": "wall clock of rr_rank on a resident matrix, median of %d" % reps}
 
 
-def batched_vs_plain(ctx, nmat=48, rmin=1000, rmax=20000, b=16, workers=16):
+def batched_vs_plain(ctx, nmat=48, rmin=1000, rmax=20000, b=16, workers=4):
     """Graph-complex-like batch (rows log-uniform, cols = rows * U(0.6, 1), 3..10
     entries +-1 per row, planted deficits): the batched engine (rr_batch_*)
     against the plain one-matrix-at-a-time GPU loop (rr_rank) on the same set."""
@@ -260,6 +260,14 @@ def batched_vs_plain(ctx, nmat=48, rmin=1000, rmax=20000, b=16, workers=16):
         drs.append(dr)
         dcs.append(dc)
         vs.append(synth.random_vectors(b, n, P, 101 + 10 * i))
+    # untimed warm-up of both modes (module loading, memory-pool growth)
+    w = list(range(0, nmat, 6))
+    wb = rr.Batch([mats[i] for i in w], b, P, [drs[i] for i in w], [dcs[i] for i in w], [vs[i] for i in w], ctx)
+    wb.ranks(workers)
+    wb.close()
+    for i in w[:2]:
+        rr.block_wiedemann_rank(rr.CsrMatrix.from_arrays(*mats[i]).to_device(P, ctx), b, P, row_precond=drs[i],
+                                col_precond=dcs[i], v=vs[i], ctx=ctx)
     t0 = time.perf_counter()
     bt = rr.Batch(mats, b, P, drs, dcs, vs, ctx)
     ranks = bt.ranks(workers)
@@ -277,7 +285,8 @@ def batched_vs_plain(ctx, nmat=48, rmin=1000, rmax=20000, b=16, workers=16):
             "note": "rows scaled from 1000-200000 to keep the run within the bench's time budget",
             "matrices": nmat, "batched_ranks_per_sec": nmat / t_batch, "plain_ranks_per_sec": nmat / t_plain,
             "batched_over_plain": t_plain / t_batch, "batched_s": t_batch, "plain_s": t_plain,
-            "timing": "wall clock, host matrices in, ranks out (upload, Krylov, generator, readout)"}
+            "timing": "wall clock, host matrices in, ranks out (upload, Krylov, generator, readout), after one "
+                  "untimed warm-up of both modes on a subset"}
 
 
 def served_stream(nreq=40, rmin=10_000, rmax=100_000, rate=50.0, b=16, seed=48):
@@ -298,6 +307,11 @@ def served_stream(nreq=40, rmin=10_000, rmax=100_000, rate=50.0, b=16, seed=48):
         dr, dc = synth.preconditioners(m, n, P, seed + 3 * i)
         reqs.append((rowptr, col, val, m, n, dr, dc, synth.random_vectors(b, n, P, seed + 3 * i + 1)))
     gaps = rng.exponential(1.0 / rate, size=nreq)
+    # untimed warm-up (contexts, module loading, memory-pool growth)
+    srv = rr.Server(b, P, lanes=4, workers=8, max_active=32, chunk_apps=64)
+    for r in reqs[:3]:
+        srv.result(srv.submit(*r[:3], r[3], r[4], *r[5:]), timeout=600.0)
+    srv.close()
     srv = rr.Server(b, P, lanes=4, workers=8, max_active=32, chunk_apps=64)
     ids = [None] * nreq
 
@@ -332,7 +346,7 @@ def served_stream(nreq=40, rmin=10_000, rmax=100_000, rate=50.0, b=16, seed=48):
             "p99_ms": st["p99_ms"], "plain_ranks_per_sec": nreq / t_plain,
             "served_over_plain": st["ranks_per_s"] / (nreq / t_plain),
             "timing": "latency = submit to rank (queueing included); throughput = completions / (last completion - "
-                      "first submit); plain = sequential upload + rr_rank per request"}
+                      "first submit); plain = sequential upload + rr_rank per request; one untimed warm-up service run"}
 
 
 def pm_basis_stage(ctx, b=16, ds=(1 << 14, 1 << 16)):
@@ -343,11 +357,15 @@ def pm_basis_stage(ctx, b=16, ds=(1 << 14, 1 << 16)):
     rng = np.random.default_rng(4)
     for d in ds:
         seq = rng.integers(0, P, size=(b * (b + 1) // 2, d + 1), dtype=np.int64).astype(np.uint32)
-        t0 = time.perf_counter()
-        rr.PM_Basis(seq, d, P, ctx)
-        out[f"d{d}_ms"] = 1e3 * (time.perf_counter() - t0)
+        best = None
+        for _ in range(2):  # the first call also grows the memory pool to this size's workspace
+            t0 = time.perf_counter()
+            rr.PM_Basis(seq, d, P, ctx)
+            dt = time.perf_counter() - t0
+            best = dt if best is None else min(best, dt)
+        out[f"d{d}_ms"] = 1e3 * best
     out["workload"] = f"pm_basis_b{b}_2b{2 * b}_uniform_random_seq"
-    out["timing"] = "wall clock of rr_pm_basis (host sequence in, generator out)"
+    out["timing"] = "wall clock of rr_pm_basis (host sequence in, generator out), best of 2"
     return out
 
 
@@ -439,6 +457,8 @@ def run_engine(args):
         "roofline": roof, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
         "matrix_setup_s": setup_s,
     }
+    ks.close()
+    dm.close()
     if rank == 0 and world == 1 and args.cpu_samples > 0:
         v, dt, threads = cpu_baseline(rowptr, col, val, m, n, b, args.cpu_samples)
         line["cpu_baseline"] = {"value": v, "unit": "GB/s", "cores": threads, "kind": "port",
@@ -449,8 +469,6 @@ def run_engine(args):
         line["batched"] = batched_vs_plain(ctx)
         line["served"] = served_stream()
         line["pm_basis"] = pm_basis_stage(ctx)
-    ks.close()
-    dm.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

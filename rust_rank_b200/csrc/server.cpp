@@ -45,6 +45,9 @@ using Clock = std::chrono::steady_clock;
 enum ReqState { kQueued, kLoading, kRunning, kSolving, kDone, kFailed };
 
 constexpr int kMaxSolveBatch = 32;  // generators solved together by one worker
+// A complete request waits up to this long for running requests of the same
+// sequence length, so that their generators are solved in one batch.
+constexpr auto kSolveWindow = std::chrono::milliseconds(100);
 
 struct Request {
   uint64_t id = 0;
@@ -63,7 +66,7 @@ struct Request {
   int64_t rank = -1;
   int status = RR_OK;
   std::string error;
-  Clock::time_point t_submit, t_done;
+  Clock::time_point t_submit, t_ready, t_done;
 };
 
 // Sequence length rule of src/main.rs:497-504.
@@ -232,7 +235,26 @@ struct rr_server_s {
       bool loading = false;
       {
         std::unique_lock<std::mutex> lk(mu);
-        cv_work.wait(lk, [&] { return stop || !tasks.empty() || !solve_q.empty(); });
+        // a complete request may be solved now unless requests of the same
+        // length are still running and its window has not run out
+        auto solvable = [&](Clock::time_point now) -> int {
+          for (size_t q = 0; q < solve_q.size(); ++q) {
+            const Request* r = reqs[solve_q[q]].get();
+            bool twin_running = false;
+            for (uint64_t id : running)
+              if (reqs[id]->apps_total == r->apps_total) { twin_running = true; break; }
+            if (!twin_running || now - r->t_ready >= kSolveWindow) return (int)q;
+          }
+          return -1;
+        };
+        int pick = -1;
+        for (;;) {
+          if (stop || !tasks.empty()) break;
+          pick = solvable(Clock::now());
+          if (pick >= 0) break;
+          if (solve_q.empty()) cv_work.wait(lk);
+          else cv_work.wait_for(lk, std::chrono::milliseconds(5));
+        }
         if (stop) break;
         if (!tasks.empty()) {  // loads first: they keep the Krylov lanes busy
           batch.push_back(reqs[tasks.front()].get());
@@ -240,8 +262,8 @@ struct rr_server_s {
           loading = true;
         } else {
           // this request and every other complete one of the same length
-          Request* r0 = reqs[solve_q.front()].get();
-          solve_q.pop_front();
+          Request* r0 = reqs[solve_q[pick]].get();
+          solve_q.erase(solve_q.begin() + pick);
           batch.push_back(r0);
           for (auto it = solve_q.begin(); it != solve_q.end() && (int)batch.size() < kMaxSolveBatch;) {
             Request* r = reqs[*it].get();
@@ -332,6 +354,7 @@ struct rr_server_s {
         for (uint64_t id : finished) {
           running.erase(std::find(running.begin(), running.end(), id));
           reqs[id]->state = kSolving;
+          reqs[id]->t_ready = Clock::now();
           solve_q.push_back(id);
           cv_work.notify_one();
         }
