@@ -1190,6 +1190,119 @@ __global__ void __launch_bounds__(kLeafThreads) pm_leaves_mma_kernel(LeafParams 
   }
 }
 
+// Block basis on the int8 tensor cores (2b <= 32): CTA (j, z) keeps column j
+// of generator z's block basis as byte planes Vp[limb][t][8 words]
+// (coefficient t = plane row, K index s = byte s) and applies
+//   V_{k+1}[t' + mask_k(i)][i] = (T_k V_k[t'])[i] 2^-32,
+// the same Montgomery convention as the CUDA-core kernel below, with exact
+// u8-limb mma.sync products (T_k staged as byte planes as in the leaves kernel).
+__device__ __forceinline__ uint32_t plane_load(const uint32_t* coeff, int NPc, int col, int row) {
+  const unsigned char* b = reinterpret_cast<const unsigned char*>(coeff);
+  const int wo = plane_word(col, row >> 2), bo = row & 3;
+  uint32_t v = 0;
+#pragma unroll
+  for (int l = 0; l < 4; ++l) v |= (uint32_t)b[4 * (l * NPc * 8 + wo) + bo] << (8 * l);
+  return v;
+}
+
+// Plane rows of the block basis kernel: K + 2 coefficients, multiple of 8.
+__host__ __device__ constexpr int bb_rows(int K) { return (K + 2 + 7) & ~7; }
+
+size_t block_basis_mma_smem_bytes(int K) { return ((size_t)2 * 4 * bb_rows(K) * 8 + 1024) * 4; }
+
+__global__ void __launch_bounds__(256) pm_block_basis_mma_kernel(const uint32_t* __restrict__ Tt,
+                                                                 const unsigned long long* __restrict__ mask,
+                                                                 const uint32_t* __restrict__ sigma_inv, int m, int K,
+                                                                 uint32_t* Mout, int64_t out_rs, int64_t out_cs,
+                                                                 int64_t out_bs, ModP M) {
+  extern __shared__ __align__(16) uint32_t bbm_smem[];
+  Tt += (int64_t)blockIdx.y * K * m * m;
+  mask += (int64_t)blockIdx.y * K;
+  sigma_inv += (int64_t)blockIdx.y * m;
+  Mout += (int64_t)blockIdx.y * out_bs;
+  const int VR = bb_rows(K);
+  uint32_t* Vc = bbm_smem;          // [4][VR][8] byte planes of V_k
+  uint32_t* Vn = Vc + 4 * VR * 8;   // V_{k+1}
+  uint32_t* Tp = Vn + 4 * VR * 8;   // [4][32][8] byte planes of T_k
+  const int j = blockIdx.x;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
+  const int g = lane >> 2, t4 = lane & 3;
+  const uint32_t p = M.p;
+  const uint32_t Wt[3] = {M.c32, (uint32_t)((uint64_t)M.c32 * 256 % p), (uint32_t)((uint64_t)M.c32 * 65536 % p)};
+  const int MT = (m + 15) / 16;
+  for (int e = tid; e < 2 * 4 * VR * 8 + 1024; e += nt) bbm_smem[e] = 0;
+  __syncthreads();
+  if (tid == 0) plane_store(Vc, VR, 0, j, 1u);  // V_0 = e_j
+  for (int k = 0; k < K; ++k) {
+    const unsigned long long mk = mask[k];
+    const uint32_t* Tk = Tt + (size_t)k * m * m;  // Tk[s * m + i] = T_k[i][s]
+    for (int e = tid; e < m * 8; e += nt) {
+      const int i = e >> 3, w = e & 7;
+      uint32_t v[4];
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj) v[jj] = (4 * w + jj < m) ? Tk[(4 * w + jj) * m + i] : 0u;
+#pragma unroll
+      for (int l = 0; l < 4; ++l) {
+        const uint32_t lo = __byte_perm(v[0], v[1], 0x40 + 0x11 * l) & 0xffffu;
+        const uint32_t hi = __byte_perm(v[2], v[3], 0x40 + 0x11 * l) & 0xffffu;
+        Tp[l * 256 + plane_word(i, w)] = lo | (hi << 16);
+      }
+    }
+    for (int e = tid; e < 4 * (k + 2) * 8; e += nt) {  // rows 0 .. k+1 of V_{k+1}
+      const int l = e / ((k + 2) * 8), r = e - l * (k + 2) * 8;
+      Vn[l * VR * 8 + r] = 0;
+    }
+    __syncthreads();
+    const int NTk = (k + 1 + 7) / 8;
+    for (int job = warp; job < MT * NTk; job += nwarps) {
+      const int mt = job / NTk, ntl = job % NTk;
+      const int r0 = mt * 16 + g, r1 = r0 + 8, col = ntl * 8 + g;
+      uint32_t A[4][4], Bf[4][2];
+#pragma unroll
+      for (int l = 0; l < 4; ++l) {
+        A[l][0] = Tp[l * 256 + plane_word(r0, t4)];
+        A[l][1] = Tp[l * 256 + plane_word(r1, t4)];
+        A[l][2] = Tp[l * 256 + plane_word(r0, t4 + 4)];
+        A[l][3] = Tp[l * 256 + plane_word(r1, t4 + 4)];
+        Bf[l][0] = Vc[l * VR * 8 + plane_word(col, t4)];
+        Bf[l][1] = Vc[l * VR * 8 + plane_word(col, t4 + 4)];
+      }
+      int C[7][4];
+#pragma unroll
+      for (int q = 0; q < 7; ++q)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) C[q][v] = 0;
+#pragma unroll
+      for (int l = 0; l < 4; ++l)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) leaf_mma_u8(C[l + r], A[l], Bf[r][0], Bf[r][1]);
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const int row = (v < 2) ? r0 : r1;
+        const int tp = ntl * 8 + 2 * t4 + (v & 1);
+        if (row < m && tp <= k) {
+          const uint64_t x = (uint64_t)(uint32_t)C[0][v] + ((uint64_t)(uint32_t)C[1][v] << 8) +
+                             ((uint64_t)(uint32_t)C[2][v] << 16) + ((uint64_t)(uint32_t)C[3][v] << 24);
+          uint32_t lo = (uint32_t)x, hi = (uint32_t)(x >> 32);
+          mac_cc((uint32_t)C[4][v], Wt[0], lo, hi);
+          mac_cc((uint32_t)C[5][v], Wt[1], lo, hi);
+          mac_cc((uint32_t)C[6][v], Wt[2], lo, hi);
+          plane_store(Vn, VR, tp + (int)((mk >> row) & 1ull), row, redc_cc(lo, hi, M));
+        }
+      }
+    }
+    __syncthreads();
+    uint32_t* tv = Vc;
+    Vc = Vn;
+    Vn = tv;
+  }
+  for (int e = tid; e < (K + 1) * m; e += nt) {
+    const int t = e / m, r = e % m;
+    Mout[(int64_t)r * out_rs + (int64_t)j * out_cs + t] = mulmod(plane_load(Vc, VR, t, r), sigma_inv[r], M);
+  }
+}
+
 // Block basis, one CTA per column j: V_0 = e_j, V_{k+1}[t][i] = T_k[i] . V_k[t - mask_k(i)]
 // (t <= k + 1), with the same Montgomery convention as the residual; then
 // Mout[i][j][t] = V_K[t][i] sigma_inv[i].  Rows are taken in the grouped slot
@@ -1467,8 +1580,14 @@ int run_base(Pm& P, MatView G, int nleaves, MatView Mout) {
   RR_CUDA(cudaGetLastError());
   // the leaves kernel indexes its transforms with the block's own K; the
   // block basis reads them with the same K
-  const size_t bsm = block_basis_smem_bytes(P.m, nleaves);
   const dim3 grid((unsigned)P.m, nb);
+  if (P.mma) {
+    pm_block_basis_mma_kernel<<<grid, 256, block_basis_mma_smem_bytes(nleaves), P.s>>>(
+        P.Tt.ptr, P.leafmask.ptr, P.sigma_inv.ptr, P.m, nleaves, Mout.p, Mout.rs, Mout.cs, Mout.bs, P.M);
+    RR_CUDA(cudaGetLastError());
+    return RR_OK;
+  }
+  const size_t bsm = block_basis_smem_bytes(P.m, nleaves);
   if (P.fold4)
     pm_block_basis_kernel<4><<<grid, 256, bsm, P.s>>>(P.Tt.ptr, P.leafmask.ptr, P.sigma_inv.ptr, P.m, nleaves, Mout.p,
                                                       Mout.rs, Mout.cs, Mout.bs, P.M);
@@ -1504,6 +1623,7 @@ int set_leaves_smem_limit(size_t bytes, size_t basis_bytes) {
   RR_CUDA(cudaFuncSetAttribute(pm_leaves_mma_kernel, attr, (int)bytes));
   RR_CUDA(cudaFuncSetAttribute(pm_block_basis_kernel<4>, attr, (int)basis_bytes));
   RR_CUDA(cudaFuncSetAttribute(pm_block_basis_kernel<2>, attr, (int)basis_bytes));
+  RR_CUDA(cudaFuncSetAttribute(pm_block_basis_mma_kernel, attr, (int)block_basis_mma_smem_bytes(64)));
   return RR_OK;
 }
 
