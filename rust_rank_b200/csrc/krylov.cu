@@ -381,7 +381,7 @@ __device__ __forceinline__ unsigned long long* seg_target(const PassParams& P, u
 template <int B, int MODE, int FE>
 // Four CTAs (32 warps) per SM: the walk is latency bound, so occupancy is
 // worth a few spilled registers (measured on the 2M x 1.5M Zipf matrix).
-__global__ void __launch_bounds__(kThreads, 4) pass_kernel(PassParams P) {
+__global__ void __launch_bounds__(kThreads, (B >= 32 ? 2 : 4)) pass_kernel(PassParams P) {
   using S = Shape<B>;
   constexpr int LPT = S::LPT, NV = S::NV, TPR = S::TPR, RPW = S::RPW;
   constexpr int NP = B * (B + 1) / 2;  // pairs in padded space

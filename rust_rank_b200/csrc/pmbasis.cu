@@ -921,15 +921,20 @@ __global__ void __launch_bounds__(kLeafThreads) pm_leaves_kernel(LeafParams P) {
 // the A fragments.  Row r of a plane keeps word w at w ^ 4 (r >> 2 & 1), so the
 // fragment loads of rows r and r + 4 fall in different banks.
 //
-// The elimination runs in one warp with one row per lane held in registers;
-// every column of the 48 is updated unconditionally (padding columns are
-// zero and stay zero), so the 48 updates of a step are independent.
+// The elimination runs in kElimWarps warps, one row per lane, each warp
+// holding kElimColsPerWarp of the 48 columns in registers; every column is
+// updated unconditionally (padding columns are zero and stay zero), so the
+// updates of a step are independent.  Two warps per SM sub-partition hide
+// each other's dependency latencies (the elimination is the serial part of a
+// leaf).
 constexpr int kMmaRows = 32;
 constexpr int kMmaCols = 16;
-constexpr int kElimWarps = 4;         // one per SM sub-partition
+constexpr int kElimWarps = 8;
 constexpr int kRpartStride = kMmaCols + 1;            // row stride of the published columns
 constexpr int kRpartSize = kMmaRows * kRpartStride;
-constexpr int kElimColsPerWarp = 12;  // 4 x 12 = 48 >= n + m
+constexpr int kElimColsPerWarp = 6;  // 8 x 6 = 48 >= n + m
+static_assert(kElimWarps * kElimColsPerWarp >= kMmaRows + kMmaCols, "elimination columns");
+static_assert(kElimWarps <= kLeafWarps, "elimination warps");
 
 // Named barrier of the elimination warps (the others wait at __syncthreads).
 __device__ __forceinline__ void elim_bar() { asm volatile("bar.sync 1, %0;" ::"n"(kElimWarps * 32) : "memory"); }
