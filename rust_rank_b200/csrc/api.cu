@@ -556,9 +556,7 @@ int rr_rank(rr_matrix* mat, int32_t b, const uint32_t* row_precond, const uint32
   std::vector<uint32_t> seq((size_t)np * stride);
   int64_t L = 0;
   RR_TRY(rr_krylov_advance(kr, max_nlen, seq.data(), stride, &L));
-  int64_t d = 1;  // src/main.rs:599-603
-  while (d <= L) d *= 2;
-  d /= 2;
+  const int64_t d = generator_order(L);
   std::vector<uint32_t> M((size_t)(2 * b) * (2 * b) * (d + 1));
   std::vector<int64_t> delta(2 * b);
   RR_TRY(rr_pm_basis(mat->ctx, seq.data(), stride, b, L, d, mat->p, M.data(), delta.data()));

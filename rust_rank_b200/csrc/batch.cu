@@ -625,21 +625,23 @@ int rr_batch_ranks(rr_batch* bt, int32_t workers, int64_t* ranks) {
   } else {
     prog.published = nmat;
   }
-  // generator jobs: runs of stack positions with equal sequence length (they
-  // finish their Krylov loops together), solved in lockstep by one batched
-  // PM-basis each, split so that a job's workspace stays within a budget
+  // generator jobs: runs of stack positions whose generators have the same
+  // order d (stack positions are sorted by sequence length, so a run is
+  // contiguous and its last position finishes its Krylov loop last), solved
+  // in lockstep by one batched PM-basis each; a job holds at most kJobMax
+  // generators and stays within a workspace budget, so that the first ones
+  // of a long run need not wait for the whole run
   struct Job { int first, count; };
   std::vector<Job> jobs;
+  auto order_of = [&](int s) { return generator_order(2 * bt->apps[s] + 1); };
   {
     constexpr size_t kJobBudget = (size_t)8 << 30;
+    constexpr int kJobMax = 16;
     for (int s0 = 0; s0 < nmat;) {
       int s1 = s0;
-      while (s1 < nmat && bt->apps[s1] == bt->apps[s0]) ++s1;
-      const int64_t L = 2 * bt->apps[s0] + 1;
-      int64_t d = 1;
-      while (d <= L) d *= 2;
-      d /= 2;
-      const int per = (int)std::max<size_t>(1, kJobBudget / pm_workspace_bytes(b, d));
+      const int64_t d = order_of(s0);
+      while (s1 < nmat && order_of(s1) == d) ++s1;
+      const int per = (int)std::min<size_t>(kJobMax, std::max<size_t>(1, kJobBudget / pm_workspace_bytes(b, d)));
       for (int q = s0; q < s1; q += per) jobs.push_back({q, std::min(per, s1 - q)});
       s0 = s1;
     }
@@ -663,27 +665,25 @@ int rr_batch_ranks(rr_batch* bt, int32_t workers, int64_t* ranks) {
         prog.cv.wait(lk, [&] { return prog.published > last || prog.failed; });
         if (prog.published <= last) break;  // the Krylov loop failed
       }
-      const int64_t L = 2 * bt->apps[first] + 1;
-      int64_t d = 1;  // src/main.rs:599-603
-      while (d <= L) d *= 2;
-      d /= 2;
+      // equal order d for the whole job; only the first d + 1 terms are read
+      const int64_t d = order_of(first), glen = d + 1;
       std::vector<std::vector<uint32_t>> seq(cnt), Mv(cnt);
       std::vector<std::vector<int64_t>> delta(cnt);
       std::vector<const uint32_t*> sp(cnt);
       std::vector<uint32_t*> mp(cnt);
       std::vector<int64_t*> dp(cnt);
-      std::vector<int64_t> strides(cnt, L);
+      std::vector<int64_t> strides(cnt, glen);
       cudaError_t e = cudaSuccess;
       if (overlap) e = cudaStreamWaitEvent(c->stream, ev[last], 0);
-      raw.resize((size_t)np * L);
+      raw.resize((size_t)np * glen);
       for (int z = 0; z < cnt && e == cudaSuccess; ++z) {
         const int s = first + z;
         e = cudaMemcpyAsync(raw.data(), bt->S.ptr + bt->s_off[s], raw.size() * 4, cudaMemcpyDeviceToHost, c->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
         if (e != cudaSuccess) break;
         seq[z].resize(raw.size());
-        for (int64_t t = 0; t < L; ++t)
-          for (int q = 0; q < np; ++q) seq[z][(size_t)q * L + t] = raw[(size_t)t * np + q];
+        for (int64_t t = 0; t < glen; ++t)
+          for (int q = 0; q < np; ++q) seq[z][(size_t)q * glen + t] = raw[(size_t)t * np + q];
         Mv[z].resize((size_t)(2 * b) * (2 * b) * (d + 1));
         delta[z].resize(2 * b);
         sp[z] = seq[z].data();

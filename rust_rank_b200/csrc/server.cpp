@@ -45,8 +45,10 @@ using Clock = std::chrono::steady_clock;
 enum ReqState { kQueued, kLoading, kRunning, kSolving, kDone, kFailed };
 
 constexpr int kMaxSolveBatch = 32;  // generators solved together by one worker
-// A complete request waits up to this long for running requests of the same
-// sequence length, so that their generators are solved in one batch.
+// A complete request waits up to this long for running requests whose
+// generators have the same order d and whose last chunks are queued, so that
+// the generators are solved in one batch (PM_Basis reads only the first d + 1
+// terms, so requests of different sequence lengths but equal d batch).
 constexpr auto kSolveWindow = std::chrono::milliseconds(100);
 
 struct Request {
@@ -61,6 +63,7 @@ struct Request {
   rr_matrix* mat = nullptr;
   rr_krylov* kr = nullptr;
   int64_t apps_total = 0, apps_queued = 0;
+  int64_t order = 0;  // generator order d of the complete sequence
   cudaEvent_t ev[2] = {nullptr, nullptr};
   int inflight = 0, ev_head = 0;  // chunks queued and not yet seen complete; oldest event
   int64_t rank = -1;
@@ -165,6 +168,7 @@ struct rr_server_s {
     RR_TRY(rr_krylov_create(r.mat, b, r.rp.data(), r.cp.data(), r.V.data(), 0, &r.kr));
     const int64_t L = max_nlen_for(r.m, r.n, b);
     r.apps_total = L / 2;  // src/main.rs:109,131: (max_nlen - 0) / 2 applications, 2 terms each
+    r.order = rr::generator_order(1 + 2 * r.apps_total);
     RR_TRY(rr::krylov_reserve(r.kr, 2 * r.apps_total + 2));
     for (auto& e : r.ev) RR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     return RR_OK;
@@ -174,7 +178,8 @@ struct rr_server_s {
   // own context, for requests of equal sequence length.
   int solve(std::vector<Request*>& rs, rr_ctx* wctx) {
     const int b = cfg.b, np = b * (b + 1) / 2, cnt = (int)rs.size();
-    const int64_t L = 1 + 2 * rs[0]->apps_total;
+    // one order d for the batch; the generator reads the first d + 1 terms
+    const int64_t d = rs[0]->order, L = d + 1;
     RR_CUDA(cudaSetDevice(device));
     // every chunk's event has completed (the scheduler saw them), so the
     // sequences are final in device memory
@@ -192,9 +197,6 @@ struct rr_server_s {
       rr_matrix_destroy(rs[z]->mat);
       rs[z]->mat = nullptr;
     }
-    int64_t d = 1;  // src/main.rs:599-603
-    while (d <= L) d *= 2;
-    d /= 2;
     std::vector<std::vector<uint32_t>> M(cnt);
     std::vector<std::vector<int64_t>> delta(cnt);
     std::vector<const uint32_t*> sp(cnt);
@@ -241,8 +243,13 @@ struct rr_server_s {
           for (size_t q = 0; q < solve_q.size(); ++q) {
             const Request* r = reqs[solve_q[q]].get();
             bool twin_running = false;
-            for (uint64_t id : running)
-              if (reqs[id]->apps_total == r->apps_total) { twin_running = true; break; }
+            for (uint64_t id : running) {
+              const Request* o = reqs[id].get();
+              if (o->order == r->order && o->apps_total - o->apps_queued <= 2 * cfg.chunk_apps) {
+                twin_running = true;
+                break;
+              }
+            }
             if (!twin_running || now - r->t_ready >= kSolveWindow) return (int)q;
           }
           return -1;
@@ -261,13 +268,13 @@ struct rr_server_s {
           tasks.pop_front();
           loading = true;
         } else {
-          // this request and every other complete one of the same length
+          // this request and every other complete one of the same order
           Request* r0 = reqs[solve_q[pick]].get();
           solve_q.erase(solve_q.begin() + pick);
           batch.push_back(r0);
           for (auto it = solve_q.begin(); it != solve_q.end() && (int)batch.size() < kMaxSolveBatch;) {
             Request* r = reqs[*it].get();
-            if (r->apps_total == r0->apps_total) {
+            if (r->order == r0->order) {
               batch.push_back(r);
               it = solve_q.erase(it);
             } else {
