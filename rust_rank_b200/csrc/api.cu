@@ -134,10 +134,14 @@ int rr_ctx_create(int device, rr_ctx** out) {
   RR_CUDA(cudaGetDeviceCount(&count));
   if (device < 0 || device >= count) return fail(RR_EINVAL, "device %d not present (%d devices)", device, count);
   RR_CUDA(cudaSetDevice(device));
-  cudaDeviceProp prop;
-  RR_CUDA(cudaGetDeviceProperties(&prop, device));
-  if (prop.major < 10)
-    return fail(RR_EUNSUPPORTED, "device %d is sm_%d%d; this build targets sm_100a", device, prop.major, prop.minor);
+  // two attributes, not cudaGetDeviceProperties: contexts are created per
+  // worker thread inside timed work, and the full property query is slow
+  int major = 0, minor = 0, sms = 0;
+  RR_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
+  RR_CUDA(cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, device));
+  RR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  if (major < 10)
+    return fail(RR_EUNSUPPORTED, "device %d is sm_%d%d; this build targets sm_100a", device, major, minor);
   {
     // keep freed stream-ordered memory in this process's pool instead of
     // returning it to the driver at every synchronisation (the generator
@@ -149,7 +153,7 @@ int rr_ctx_create(int device, rr_ctx** out) {
   }
   std::unique_ptr<rr_ctx> c(new rr_ctx);
   c->device = device;
-  c->num_sms = prop.multiProcessorCount;
+  c->num_sms = sms;
   RR_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   *out = c.release();
   return RR_OK;
