@@ -186,3 +186,32 @@ def test_live_reference_harness_if_built():
             ln = C.c_int64()
             R.ref_pm_basis(np.ascontiguousarray(seq, np.uint64), b, nlen, nlen, d, P_SMALL, Mr, dr, C.byref(ln))
             assert np.array_equal(M, Mr) and np.array_equal(delta, dr)
+
+
+@pytest.mark.parametrize("b,nlen", [(2, 45), (3, 70), (4, 33)])
+def test_pm_basis_reads_only_first_d_plus_1_terms(b, nlen):
+    """PM_Basis(seq, d) depends on the first d + 1 terms only (M_Basis uses
+    coefficient 0 and every product of _PM_Basis is truncated to d + 1
+    coefficients, src/sigma_basis.rs:198,205).  The batched engine and the
+    rank service rely on this to solve generators of equal order d together
+    whatever their sequence lengths."""
+    p = 2013265921
+    rng = np.random.default_rng(b * 1000 + nlen)
+    seq = rng.integers(0, p, size=(b * (b + 1) // 2, nlen), dtype=np.int64).astype(np.uint32)
+    d = 1
+    while d <= nlen:
+        d *= 2
+    d //= 2
+    M_full, delta_full = oracle.pm_basis(seq, b, d, p)
+    M_cut, delta_cut = oracle.pm_basis(seq[:, : d + 1], b, d, p)
+    assert np.array_equal(M_full, M_cut) and np.array_equal(delta_full, delta_cut)
+    # a change beyond term d changes nothing (term d itself is not read
+    # either: the deepest leaf of the second half sees coefficient d - 1); a
+    # change at term d - 1 does
+    other = seq.copy()
+    other[:, d:] = rng.integers(0, p, size=(other.shape[0], nlen - d), dtype=np.int64).astype(np.uint32)
+    M_o, _ = oracle.pm_basis(other, b, d, p)
+    assert np.array_equal(M_full, M_o)
+    other[0, d - 1] = (int(other[0, d - 1]) + 1) % p
+    M_d, _ = oracle.pm_basis(other, b, d, p)
+    assert not np.array_equal(M_full, M_d)
