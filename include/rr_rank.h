@@ -151,6 +151,23 @@ int rr_pm_basis_short_noalloc(const uint32_t* d_seq, int64_t seq_stride, int32_t
 int rr_rank_from_basis(const uint32_t* M, const int64_t* delta, int32_t b, int64_t len, uint32_t p,
                        int64_t* rank);
 
+/* is_generating_poly (src/blockbmtest.rs:445-461): *is_gen = 1 iff for every
+ * l in [0, N - k) the matrix sum_{i<k} seq[l+i] * poly[i] is zero mod p.
+ * poly [k][n][n], seq [N][n][n], row-major, entries in [0, p).  N < k is
+ * RR_EINVAL (the reference's range 0..N-k has no meaning there).  Host code,
+ * spread over the host's threads. */
+int rr_is_generating_poly(const uint32_t* poly, int64_t k, const uint32_t* seq, int64_t N, int32_t n, uint32_t p,
+                          int32_t* is_gen);
+
+/* Scalar Berlekamp-Massey, the call surface of block_berlekamp_massey at
+ * block width 1 (src/block_berlekamp_massey.rs:104-131, which hands seq[0] to
+ * bubblemath 0.1.2's linear_recurrence::berlekamp_massey; that crate is not
+ * part of the reference tree, so its output convention is not pinned here).
+ * Returns Massey's connection polynomial of the shortest linear recurrence of
+ * seq[0..n): conn[0] = 1, conn[0..L], sum_{i=0..L} conn[i] seq[j-i] = 0 mod p
+ * for L <= j < n.  conn needs room for n + 1 entries.  Host code. */
+int rr_berlekamp_massey(const uint32_t* seq, int64_t n, uint32_t p, uint32_t* conn, int64_t* L);
+
 /* rr_pm_basis for `count` sequences with the same b, d and p, solved in
  * lockstep on the device (one launch per step of the recursion for all of
  * them); seqs[z] is [b(b+1)/2][seq_strides[z] >= nlen], M[z] and delta[z] as

@@ -47,7 +47,8 @@ def _close_all():
 
 __all__ = ["Context", "CsrMatrix", "DeviceMatrix", "KrylovStream", "main_loop_s_mt2", "PM_Basis",
            "analyze_pm_basis", "block_wiedemann_rank", "save_wdm_file_sym", "load_wdm_file_sym",
-           "default_max_nlen", "Batch", "Server", "RRError"]
+           "default_max_nlen", "Batch", "Server", "RRError", "is_generating_poly", "berlekamp_massey",
+           "block_berlekamp_massey"]
 
 DEFAULT_PRIME = 2013265921
 
@@ -321,6 +322,40 @@ def analyze_pm_basis(basis: np.ndarray, delta: np.ndarray, p: int) -> int:
     r = C.c_int64()
     check(lib().rr_rank_from_basis(ptr(basis), ptr(delta), basis.shape[0] // 2, basis.shape[2], p, C.byref(r)))
     return r.value
+
+
+def is_generating_poly(poly, seq, p: int) -> bool:
+    """src/blockbmtest.rs:445-461: whether sum_{i<k} seq[l+i] @ poly[i] == 0 mod p for
+    every l in [0, N - k).  poly: k matrices n x n, seq: N matrices n x n (residues)."""
+    poly = np.ascontiguousarray(np.asarray(poly, dtype=np.int64) % p, np.uint32)
+    seq = np.ascontiguousarray(np.asarray(seq, dtype=np.int64) % p, np.uint32)
+    if poly.ndim != 3 or seq.ndim != 3 or poly.shape[1:] != seq.shape[1:] or poly.shape[1] != poly.shape[2]:
+        raise ValueError("poly and seq must be stacks of equal square matrices")
+    ok = C.c_int32()
+    check(lib().rr_is_generating_poly(ptr(poly), poly.shape[0], ptr(seq), seq.shape[0], poly.shape[1], p,
+                                      C.byref(ok)))
+    return bool(ok.value)
+
+
+def berlekamp_massey(seq, p: int) -> np.ndarray:
+    """Shortest linear recurrence of a scalar sequence mod p (Massey's algorithm):
+    the connection polynomial [1, c_1, ..., c_L] with sum_i c_i seq[j - i] = 0 for j >= L."""
+    s = np.ascontiguousarray(np.asarray(seq, dtype=np.int64) % p, np.uint32)
+    conn = np.zeros(s.size + 1, np.uint32)
+    L = C.c_int64()
+    check(lib().rr_berlekamp_massey(ptr(s), s.size, p, ptr(conn), C.byref(L)))
+    return conn[: L.value + 1].copy()
+
+
+def block_berlekamp_massey(seq, num_u: int, num_v: int, p: int) -> np.ndarray:
+    """The call surface of src/block_berlekamp_massey.rs:104-131: only block width 1
+    is implemented (as in the reference, which warns and uses seq[0] otherwise); the
+    scalar sequence seq[0] goes to berlekamp_massey."""
+    if num_u > 1 or num_v > 1:
+        import warnings
+
+        warnings.warn("Matrix Berlekamp-Massey is not implemented; using the first sequence only", stacklevel=2)
+    return berlekamp_massey(np.asarray(seq[0]), p).astype(np.uint64)
 
 
 def block_wiedemann_rank(a: CsrMatrix | DeviceMatrix, num_v: int, theprime: int = DEFAULT_PRIME,

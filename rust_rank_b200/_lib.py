@@ -48,6 +48,8 @@ SIGNATURES = {
     "rr_pm_basis": (C.c_int, [_vp, _vp, _i64, _i32, _i64, _i64, _u32, _vp, _vp]),
     "rr_pm_basis_short_noalloc": (C.c_int, [_vp, _i64, _i32, _i64, _i64, _u32, _vp, _vp, _vp]),
     "rr_rank_from_basis": (C.c_int, [_vp, _vp, _i32, _i64, _u32, _pi64]),
+    "rr_is_generating_poly": (C.c_int, [_vp, _i64, _vp, _i64, _i32, _u32, C.POINTER(C.c_int32)]),
+    "rr_berlekamp_massey": (C.c_int, [_vp, _i64, _u32, _vp, _pi64]),
     "rr_pm_basis_batch": (C.c_int, [_vp, _i32, _vp, _vp, _i32, _i64, _i64, _u32, _vp, _vp]),
     "rr_rank": (C.c_int, [_vp, _i32, _vp, _vp, _vp, _i64, _pi64]),
     "rr_batch_create": (C.c_int, [_vp, _i32, _vp, _vp, _vp, _vp, _vp, _u32, _i32, _vp, _vp, _vp, C.POINTER(_vp)]),
