@@ -451,7 +451,7 @@ def run_engine(args):
     t0 = time.perf_counter()
     ks2 = rr.KrylovStream(dm, Vp, drp, dcp, 0)
     L = ks2.advance(2 * args.steps, seq)
-    curv_out[:] = ks2.get_curv()
+    ks2.get_curv(out=curv_out)
     e2e_s = time.perf_counter() - t0
     e2e_s = max_over_ranks(e2e_s, world)
     assert L == 2 * args.steps + 1

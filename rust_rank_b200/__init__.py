@@ -193,8 +193,13 @@ class KrylovStream:
     def fill_status(self) -> str:
         return "device"
 
-    def get_curv(self) -> np.ndarray:
-        out = np.zeros((self.b, self.n), np.uint32)
+    def get_curv(self, out: np.ndarray | None = None) -> np.ndarray:
+        """The current block w_k, [b][n] in the caller's column order.  `out`: a
+        C-contiguous uint32 [b][n] array to write into (e.g. pinned host memory)."""
+        if out is None:
+            out = np.empty((self.b, self.n), np.uint32)
+        elif out.dtype != np.uint32 or out.shape != (self.b, self.n) or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a C-contiguous uint32 array of shape {(self.b, self.n)}")
         check(lib().rr_krylov_get_curv(self.handle, ptr(out)))
         return out
 

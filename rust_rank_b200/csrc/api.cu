@@ -235,12 +235,15 @@ int rr_krylov_create(rr_matrix* mat, int32_t b, const uint32_t* row_precond, con
   if (seq_len < 0) return fail(RR_EINVAL, "seq_len < 0");
   const uint32_t p = mat->p;
   const int64_t m = mat->m, n = mat->n;
-  for (int64_t i = 0; i < m; ++i)
-    if (row_precond[i] == 0 || row_precond[i] >= p) return fail(RR_EINVAL, "row_precond[%lld] not in [1, p)", (long long)i);
-  for (int64_t i = 0; i < n; ++i)
-    if (col_precond[i] == 0 || col_precond[i] >= p) return fail(RR_EINVAL, "col_precond[%lld] not in [1, p)", (long long)i);
-  for (int64_t i = 0; i < (int64_t)b * n; ++i)
-    if (curv[i] >= p) return fail(RR_EINVAL, "curv entry %lld not reduced mod p", (long long)i);
+  // input checks on the host's cores (the first offending index is reported)
+  {
+    int64_t i = host_first_index(m, [&](int64_t k) { return row_precond[k] == 0 || row_precond[k] >= p; });
+    if (i < m) return fail(RR_EINVAL, "row_precond[%lld] not in [1, p)", (long long)i);
+    i = host_first_index(n, [&](int64_t k) { return col_precond[k] == 0 || col_precond[k] >= p; });
+    if (i < n) return fail(RR_EINVAL, "col_precond[%lld] not in [1, p)", (long long)i);
+    i = host_first_index((int64_t)b * n, [&](int64_t k) { return curv[k] >= p; });
+    if (i < (int64_t)b * n) return fail(RR_EINVAL, "curv entry %lld not reduced mod p", (long long)i);
+  }
   rr_ctx* ctx = mat->ctx;
   RR_CUDA(cudaSetDevice(ctx->device));
   cudaStream_t s = ctx->stream;
@@ -255,28 +258,57 @@ int rr_krylov_create(rr_matrix* mat, int32_t b, const uint32_t* row_precond, con
     const unsigned __int128 q = (unsigned __int128)(p - 1) * (p - 1);
     kr->fold4 = (F + 4 * q) < ((unsigned __int128)1 << 64);
   }
-  // preconditioners in device order; D_c^{-1} by one inversion and prefix products
-  std::vector<uint32_t> dr(m), dc(n), dci(n);
-  for (int64_t i = 0; i < m; ++i) dr[i] = row_precond[mat->rowperm[i]];
-  for (int64_t i = 0; i < n; ++i) dc[i] = col_precond[mat->colperm[i]];
+  // preconditioners in device order, in the forms the epilogues use:
+  // d_r R^2, d_c R^2, d_c R and d_c^{-1} (all mod p), on the host's cores
+  const uint64_t R1 = kr->M.r1, R2 = R1 * R1 % p;
+  std::vector<uint32_t> dr(m), dc(n), dcr(n), dci(n);
+  host_parallel_ranges(m, (int64_t)1 << 16, [&](int64_t lo, int64_t hi) {
+    for (int64_t i = lo; i < hi; ++i) dr[i] = (uint32_t)((uint64_t)row_precond[mat->rowperm[i]] * R2 % p);
+  });
+  host_parallel_ranges(n, (int64_t)1 << 16, [&](int64_t lo, int64_t hi) {
+    for (int64_t i = lo; i < hi; ++i) dc[i] = col_precond[mat->colperm[i]];
+  });
   {
-    std::vector<uint32_t> pre(n + 1);
-    pre[0] = 1;
-    for (int64_t i = 0; i < n; ++i) pre[i + 1] = (uint32_t)((uint64_t)pre[i] * dc[i] % p);
-    uint64_t inv = host_invmod(pre[n], p);
-    for (int64_t i = n - 1; i >= 0; --i) {
-      dci[i] = (uint32_t)(inv * pre[i] % p);
-      inv = inv * dc[i] % p;
-    }
+    // D_c^{-1} by batch inversion in blocks: prefix products per block, one
+    // Fermat inversion per block total, then each block walked backwards
+    const int64_t nblk = std::max<int64_t>(1, std::min<int64_t>(64, n >> 15));
+    std::vector<uint32_t> pre(n), tot(nblk), itot(nblk);
+    auto blk = [&](int64_t t, int64_t& lo, int64_t& hi) {
+      lo = n * t / nblk;
+      hi = n * (t + 1) / nblk;
+    };
+    host_parallel_ranges(nblk, 1, [&](int64_t t0, int64_t t1) {
+      for (int64_t t = t0; t < t1; ++t) {
+        int64_t lo, hi;
+        blk(t, lo, hi);
+        uint64_t acc = 1;
+        for (int64_t i = lo; i < hi; ++i) {
+          pre[i] = (uint32_t)acc;  // product of the block's entries before i
+          acc = acc * dc[i] % p;
+        }
+        tot[t] = (uint32_t)acc;
+      }
+    });
+    for (int64_t t = 0; t < nblk; ++t) itot[t] = host_invmod(tot[t], p);
+    host_parallel_ranges(nblk, 1, [&](int64_t t0, int64_t t1) {
+      for (int64_t t = t0; t < t1; ++t) {
+        int64_t lo, hi;
+        blk(t, lo, hi);
+        uint64_t inv = itot[t];
+        for (int64_t i = hi - 1; i >= lo; --i) {
+          dci[i] = (uint32_t)(inv * pre[i] % p);
+          inv = inv * dc[i] % p;
+        }
+      }
+    });
   }
-  {
-    const uint64_t R1 = kr->M.r1, R2 = R1 * R1 % p;
-    std::vector<uint32_t> dcr(n);
-    for (int64_t i = 0; i < m; ++i) dr[i] = (uint32_t)(dr[i] * R2 % p);
-    for (int64_t i = 0; i < n; ++i) {
-      dcr[i] = (uint32_t)(dc[i] * R1 % p);
-      dc[i] = (uint32_t)(dc[i] * R2 % p);
+  host_parallel_ranges(n, (int64_t)1 << 16, [&](int64_t lo, int64_t hi) {
+    for (int64_t i = lo; i < hi; ++i) {
+      dcr[i] = (uint32_t)((uint64_t)dc[i] * R1 % p);
+      dc[i] = (uint32_t)((uint64_t)dc[i] * R2 % p);
     }
+  });
+  {
     RR_TRY(kr->dr_m.alloc_async(m, s));
     RR_TRY(kr->dc_m.alloc_async(n, s));
     RR_TRY(kr->dc_r.alloc_async(n, s));

@@ -2,9 +2,12 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <atomic>
 #include <cstdarg>
 #include <cstdint>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "rr_modp.cuh"
@@ -34,6 +37,38 @@ ModP make_modp(uint32_t p);
 bool is_prime_u32(uint32_t p);
 uint32_t host_powmod(uint32_t a, uint64_t e, uint32_t p);
 uint32_t host_invmod(uint32_t a, uint32_t p);
+
+// fn(lo, hi) over contiguous ranges covering [0, n), run on the host's cores
+// (ranges of at least `grain` elements; one range, on the calling thread,
+// when n is small).
+template <class F>
+inline void host_parallel_ranges(int64_t n, int64_t grain, F fn) {
+  const int64_t hw = std::max(1u, std::thread::hardware_concurrency());
+  const int64_t nt = std::max<int64_t>(1, std::min<int64_t>(hw, n / std::max<int64_t>(grain, 1)));
+  if (nt == 1) {
+    if (n > 0) fn((int64_t)0, n);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (int64_t t = 0; t < nt; ++t) pool.emplace_back([&fn, n, nt, t] { fn(n * t / nt, n * (t + 1) / nt); });
+  for (auto& th : pool) th.join();
+}
+
+// Smallest i < n with bad(i), or n; scanned on the host's cores.
+template <class F>
+inline int64_t host_first_index(int64_t n, F bad) {
+  std::atomic<int64_t> first{n};
+  host_parallel_ranges(n, (int64_t)1 << 16, [&](int64_t lo, int64_t hi) {
+    for (int64_t i = lo; i < hi && i < first.load(std::memory_order_relaxed); ++i)
+      if (bad(i)) {
+        int64_t cur = first.load();
+        while (i < cur && !first.compare_exchange_weak(cur, i)) {
+        }
+        break;
+      }
+  });
+  return first.load();
+}
 
 // Owning device buffer.
 template <class T>
