@@ -64,6 +64,7 @@ ModP make_modp(uint32_t p) {
 }
 
 int launch_scatter_block(rr_krylov* kr, const uint32_t* d_V, uint32_t* d_out);
+int launch_precond(rr_krylov* kr, const uint32_t* d_rp, const uint32_t* d_cp, const int32_t* d_rowperm);
 
 }  // namespace rr
 
@@ -259,66 +260,23 @@ int rr_krylov_create(rr_matrix* mat, int32_t b, const uint32_t* row_precond, con
     kr->fold4 = (F + 4 * q) < ((unsigned __int128)1 << 64);
   }
   // preconditioners in device order, in the forms the epilogues use:
-  // d_r R^2, d_c R^2, d_c R and d_c^{-1} (all mod p), on the host's cores
-  const uint64_t R1 = kr->M.r1, R2 = R1 * R1 % p;
-  std::vector<uint32_t> dr(m), dc(n), dcr(n), dci(n);
-  host_parallel_ranges(m, (int64_t)1 << 16, [&](int64_t lo, int64_t hi) {
-    for (int64_t i = lo; i < hi; ++i) dr[i] = (uint32_t)((uint64_t)row_precond[mat->rowperm[i]] * R2 % p);
-  });
-  host_parallel_ranges(n, (int64_t)1 << 16, [&](int64_t lo, int64_t hi) {
-    for (int64_t i = lo; i < hi; ++i) dc[i] = col_precond[mat->colperm[i]];
-  });
+  // d_r R^2, d_c R^2, d_c R and d_c^{-1} (all mod p), computed on the device
+  // from the caller's arrays and the row renumbering
   {
-    // D_c^{-1} by batch inversion in blocks: prefix products per block, one
-    // Fermat inversion per block total, then each block walked backwards
-    const int64_t nblk = std::max<int64_t>(1, std::min<int64_t>(64, n >> 15));
-    std::vector<uint32_t> pre(n), tot(nblk), itot(nblk);
-    auto blk = [&](int64_t t, int64_t& lo, int64_t& hi) {
-      lo = n * t / nblk;
-      hi = n * (t + 1) / nblk;
-    };
-    host_parallel_ranges(nblk, 1, [&](int64_t t0, int64_t t1) {
-      for (int64_t t = t0; t < t1; ++t) {
-        int64_t lo, hi;
-        blk(t, lo, hi);
-        uint64_t acc = 1;
-        for (int64_t i = lo; i < hi; ++i) {
-          pre[i] = (uint32_t)acc;  // product of the block's entries before i
-          acc = acc * dc[i] % p;
-        }
-        tot[t] = (uint32_t)acc;
-      }
-    });
-    for (int64_t t = 0; t < nblk; ++t) itot[t] = host_invmod(tot[t], p);
-    host_parallel_ranges(nblk, 1, [&](int64_t t0, int64_t t1) {
-      for (int64_t t = t0; t < t1; ++t) {
-        int64_t lo, hi;
-        blk(t, lo, hi);
-        uint64_t inv = itot[t];
-        for (int64_t i = hi - 1; i >= lo; --i) {
-          dci[i] = (uint32_t)(inv * pre[i] % p);
-          inv = inv * dc[i] % p;
-        }
-      }
-    });
-  }
-  host_parallel_ranges(n, (int64_t)1 << 16, [&](int64_t lo, int64_t hi) {
-    for (int64_t i = lo; i < hi; ++i) {
-      dcr[i] = (uint32_t)((uint64_t)dc[i] * R1 % p);
-      dc[i] = (uint32_t)((uint64_t)dc[i] * R2 % p);
-    }
-  });
-  {
+    DevBuf<uint32_t> rp, cp;
+    DevBuf<int32_t> rperm;
+    RR_TRY(rp.alloc_async(std::max<int64_t>(m, 1), s));
+    RR_TRY(cp.alloc_async(std::max<int64_t>(n, 1), s));
+    RR_TRY(rperm.alloc_async(std::max<int64_t>(m, 1), s));
     RR_TRY(kr->dr_m.alloc_async(m, s));
     RR_TRY(kr->dc_m.alloc_async(n, s));
     RR_TRY(kr->dc_r.alloc_async(n, s));
     RR_TRY(kr->dcinv.alloc_async(n, s));
-    RR_CUDA(cudaMemcpyAsync(kr->dr_m.ptr, dr.data(), m * 4, cudaMemcpyHostToDevice, s));
-    RR_CUDA(cudaMemcpyAsync(kr->dc_m.ptr, dc.data(), n * 4, cudaMemcpyHostToDevice, s));
-    RR_CUDA(cudaMemcpyAsync(kr->dc_r.ptr, dcr.data(), n * 4, cudaMemcpyHostToDevice, s));
-    RR_CUDA(cudaMemcpyAsync(kr->dcinv.ptr, dci.data(), n * 4, cudaMemcpyHostToDevice, s));
-    RR_CUDA(cudaStreamSynchronize(s));  // host vectors die at scope end
-  }
+    RR_CUDA(cudaMemcpyAsync(rp.ptr, row_precond, m * 4, cudaMemcpyHostToDevice, s));
+    RR_CUDA(cudaMemcpyAsync(cp.ptr, col_precond, n * 4, cudaMemcpyHostToDevice, s));
+    RR_CUDA(cudaMemcpyAsync(rperm.ptr, mat->rowperm.data(), m * 4, cudaMemcpyHostToDevice, s));
+    RR_TRY(launch_precond(kr.get(), rp.ptr, cp.ptr, rperm.ptr));
+  }  // the staging buffers are freed in stream order, after the kernel
   const int B = kr->B;
   RR_TRY(kr->X[0].alloc_async((size_t)n * B, s));
   RR_TRY(kr->X[1].alloc_async((size_t)n * B, s));

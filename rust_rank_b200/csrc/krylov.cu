@@ -947,6 +947,42 @@ int krylov_launch_get_curv(rr_krylov* kr, uint32_t* d_out) {
   return RR_OK;
 }
 
+// The preconditioners in device order and in the forms the epilogues use:
+// d_r R^2, d_c R^2, d_c R and d_c^{-1} (mod p; the inverse by Fermat, p prime).
+__global__ void precond_kernel(const uint32_t* __restrict__ rp, const uint32_t* __restrict__ cp,
+                               const int32_t* __restrict__ rowperm, const int32_t* __restrict__ colperm, int64_t m,
+                               int64_t n, uint32_t R1, uint32_t R2, ModP M, uint32_t* __restrict__ dr_m,
+                               uint32_t* __restrict__ dc_m, uint32_t* __restrict__ dc_r, uint32_t* __restrict__ dcinv) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m + n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (i < m) {
+      dr_m[i] = mulmod(rp[rowperm[i]], R2, M);
+    } else {
+      const int64_t j = i - m;
+      const uint32_t c = cp[colperm[j]];
+      dc_m[j] = mulmod(c, R2, M);
+      dc_r[j] = mulmod(c, R1, M);
+      uint32_t r = 1, a = c;
+      for (uint32_t e = M.p - 2; e; e >>= 1) {
+        if (e & 1) r = mulmod(r, a, M);
+        a = mulmod(a, a, M);
+      }
+      dcinv[j] = r;
+    }
+  }
+}
+
+int launch_precond(rr_krylov* kr, const uint32_t* d_rp, const uint32_t* d_cp, const int32_t* d_rowperm) {
+  const int64_t m = kr->mat->m, n = kr->mat->n;
+  const uint64_t p = kr->M.p, R1 = kr->M.r1, R2 = R1 * R1 % p;
+  const int threads = 256;
+  const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((m + n + threads - 1) / threads, 4 * 148 * 8));
+  precond_kernel<<<blocks, threads, 0, kr->mat->ctx->stream>>>(d_rp, d_cp, d_rowperm, kr->mat->d_colperm.ptr, m, n,
+                                                               (uint32_t)R1, (uint32_t)R2, kr->M, kr->dr_m.ptr,
+                                                               kr->dc_m.ptr, kr->dc_r.ptr, kr->dcinv.ptr);
+  RR_CUDA(cudaGetLastError());
+  return RR_OK;
+}
+
 int launch_scatter_block(rr_krylov* kr, const uint32_t* d_V, uint32_t* d_out) {
   const int64_t n = kr->mat->n;
   const int threads = 256;
