@@ -146,3 +146,27 @@ def test_invalid_arguments_fail_loudly(ctx):
     dc0[3] = 0
     with pytest.raises(rr.RRError):
         rr.KrylovStream(dm, np.zeros((2, n), np.uint32), dr, dc0)
+
+
+def test_two_runs_are_identical(ctx):
+    """Determinism of two GPU runs (the reference checks it for its GPU
+    products, cuda_test/cupoly_mat_mul.h:638-690): sequence and generator of
+    the same inputs, computed twice, are bit-identical (the arithmetic is
+    exact, so no reduction order can change them)."""
+    rowptr, col, val, m, n = synth.plain_single(n=3000, k=6, dep_rows=50, p=P, seed=17)
+    b = 16
+    dr, dc = synth.preconditioners(m, n, P, 18)
+    V = synth.random_vectors(b, n, P, 19)
+    L = rr.default_max_nlen(m, n, b)
+    runs = []
+    for _ in range(2):
+        s, cv, ks = gpu_sequence(ctx, rowptr, col, val, m, n, P, dr, dc, V, L)
+        ks.close()
+        d = 1
+        while d <= s.shape[1]:
+            d *= 2
+        d //= 2
+        M, delta = rr.PM_Basis(s, d, P, ctx)
+        runs.append((s, cv, M, delta))
+    for a, b_ in zip(runs[0], runs[1]):
+        assert np.array_equal(a, b_)
