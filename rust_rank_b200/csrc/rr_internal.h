@@ -211,10 +211,11 @@ int pm_basis_batch_device(rr_ctx* ctx, int nb, const uint32_t* const* seqs, cons
 // Device bytes pm_basis_batch_device needs per generator.
 size_t pm_workspace_bytes(int b, int64_t d);
 // Order d of the generator computed from a sequence of nlen terms: the largest
-// power of two <= nlen (src/main.rs:598-603).  PM_Basis reads only the first
-// d + 1 terms (M_Basis uses coefficient 0, src/sigma_basis.rs:198, and every
-// product is truncated to d + 1 coefficients, src/sigma_basis.rs:205), so
-// sequences of different lengths with equal d are solved in one batch.
+// power of two <= nlen (src/main.rs:598-603).  PM_Basis of order d reads only
+// the first d terms (M_Basis uses coefficient 0, src/sigma_basis.rs:198, and
+// every product is truncated to d + 1 coefficients, src/sigma_basis.rs:205, of
+// which the deepest leaf sees coefficient d - 1), so sequences of different
+// lengths with equal d are solved in one batch.
 inline int64_t generator_order(int64_t nlen) {
   int64_t d = 1;
   while (d <= nlen) d *= 2;

@@ -15,8 +15,9 @@
 //              lanes and overlap on the device
 //   solving -> once its sequence is complete a worker thread copies it out
 //              and solves the generator on a stream of its own, together
-//              with the other complete requests of the same sequence length
-//              (one batched PM-basis, generators in lockstep), reads off the
+//              with the other complete requests whose generators have the
+//              same order d (one batched PM-basis, generators in lockstep),
+//              reads off the
 //              rank (rr_rank_from_basis) and frees the request's device
 //              memory, which admits the next requests
 //   done
@@ -47,8 +48,8 @@ enum ReqState { kQueued, kLoading, kRunning, kSolving, kDone, kFailed };
 constexpr int kMaxSolveBatch = 32;  // generators solved together by one worker
 // A complete request waits up to this long for running requests whose
 // generators have the same order d and whose last chunks are queued, so that
-// the generators are solved in one batch (PM_Basis reads only the first d + 1
-// terms, so requests of different sequence lengths but equal d batch).
+// the generators are solved in one batch (PM_Basis of order d reads only the
+// first d terms, so requests of different sequence lengths but equal d batch).
 constexpr auto kSolveWindow = std::chrono::milliseconds(100);
 
 struct Request {
