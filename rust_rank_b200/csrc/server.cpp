@@ -26,6 +26,7 @@
 // (sequence length rule of src/main.rs:497-504, PM-basis with d = largest
 // power of two <= length), so its rank does not depend on what else runs.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
@@ -63,7 +64,10 @@ struct Request {
   int lane = 0;
   rr_matrix* mat = nullptr;
   rr_krylov* kr = nullptr;
-  int64_t apps_total = 0, apps_queued = 0;
+  int64_t apps_total = 0;
+  // advanced by the scheduler without the service lock, read by workers
+  // under it (the solve-batching window looks at running requests)
+  std::atomic<int64_t> apps_queued{0};
   int64_t order = 0;  // generator order d of the complete sequence
   cudaEvent_t ev[2] = {nullptr, nullptr};
   int inflight = 0, ev_head = 0;  // chunks queued and not yet seen complete; oldest event
