@@ -242,8 +242,8 @@ struct rr_server_s {
       bool loading = false;
       {
         std::unique_lock<std::mutex> lk(mu);
-        // a complete request may be solved now unless requests of the same
-        // length are still running and its window has not run out
+        // a complete request may be solved now unless a running request of
+        // the same order is about to complete and its window has not run out
         auto solvable = [&](Clock::time_point now) -> int {
           for (size_t q = 0; q < solve_q.size(); ++q) {
             const Request* r = reqs[solve_q[q]].get();
