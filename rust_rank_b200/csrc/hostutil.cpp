@@ -186,7 +186,10 @@ int rr_wdm_load(const char* path, int64_t* m, int64_t* n, uint32_t* p, int32_t* 
 
 // src/matrices.rs:662-732: "%" comments and blank lines skipped; the first
 // 3-field line is the header; entries with a non-positive index are skipped;
-// values are reduced mod p with the sign handled as in the reference.
+// values are reduced mod p with the sign handled as in the reference.  The
+// reference expects the entries sorted by row; here they are grouped by row
+// with a stable counting sort, so a row-sorted file gives the same CSR and an
+// unsorted one still gives a valid matrix.
 int rr_sms_load(const char* path, uint32_t p, int64_t* m, int64_t* n, int64_t* nnz, int64_t* rowptr, int32_t* col,
                 uint32_t* val) {
   if (!path || !m || !n || !nnz) return fail(RR_EINVAL, "NULL argument");
@@ -199,8 +202,6 @@ int rr_sms_load(const char* path, uint32_t p, int64_t* m, int64_t* n, int64_t* n
   std::vector<int64_t> rows;
   std::vector<int32_t> cols;
   std::vector<uint32_t> vals;
-  int64_t last_row = -1;
-  bool sorted = true;
   while (read_line(F.f, line)) {
     size_t a = line.find_first_not_of(" \t\r");
     if (a == std::string::npos || line[a] == '%') continue;
@@ -219,8 +220,6 @@ int rr_sms_load(const char* path, uint32_t p, int64_t* m, int64_t* n, int64_t* n
     if (r > hm || c > hn) return fail(RR_EIO, "%s: entry (%lld, %lld) outside %lld x %lld", path, r, c, hm, hn);
     long long v = x % (long long)p;
     if (v < 0) v += p;
-    if (r - 1 < last_row) sorted = false;
-    last_row = r - 1;
     rows.push_back(r - 1);
     cols.push_back((int32_t)(c - 1));
     vals.push_back((uint32_t)v);
@@ -242,7 +241,6 @@ int rr_sms_load(const char* path, uint32_t p, int64_t* m, int64_t* n, int64_t* n
     col[pos] = cols[k];
     val[pos] = vals[k];
   }
-  (void)sorted;
   return RR_OK;
 }
 

@@ -112,3 +112,35 @@ def test_default_sequence_length_rule():
     assert rr.default_max_nlen(182, 168, 1) == 340
     assert rr.default_max_nlen(182, 168, 4) == 128
     assert rr.default_max_nlen(20000, 20000, 8) == 8192
+
+
+def test_sms_loader_edge_cases(tmp_path):
+    p = 2013265921
+    # comments, blank lines, a non-positive index (skipped), negative values,
+    # rows out of order (grouped by row, file order kept inside a row)
+    text = "% header next\n\n3 4 M\n2 1 -1\n1 4 5\n0 2 9\n2 3 -7\n1 1 2\n3 2 1\n0 0 0\n"
+    (tmp_path / "a.sms").write_text(text)
+    a = rr.CsrMatrix.load_csr_matrix_from_sms(str(tmp_path / "a.sms"), p)
+    assert (a.n_rows, a.n_cols) == (3, 4)
+    assert a.row_ptr.tolist() == [0, 2, 4, 5]
+    assert a.col_indices.tolist() == [3, 0, 0, 2, 1]
+    assert a.values.tolist() == [5, 2, p - 1, p - 7, 1]
+    # an entry outside the declared shape, and a file without a header line
+    (tmp_path / "b.sms").write_text("2 2 M\n3 1 1\n")
+    with pytest.raises(rr.RRError) as e:
+        rr.CsrMatrix.load_csr_matrix_from_sms(str(tmp_path / "b.sms"), p)
+    assert "outside" in str(e.value)
+    (tmp_path / "c.sms").write_text("% only a comment\n")
+    with pytest.raises(rr.RRError):
+        rr.CsrMatrix.load_csr_matrix_from_sms(str(tmp_path / "c.sms"), p)
+
+
+def test_rank_readout_rejects_bad_degrees():
+    b, len_ = 2, 5
+    M = np.zeros((2 * b, 2 * b, len_), np.uint32)
+    with pytest.raises(rr.RRError):  # -delta beyond the basis length
+        rr.analyze_pm_basis(M, np.array([-len_, 0, 0, 0], np.int64), 3323)
+    with pytest.raises(rr.RRError) as e:  # degree 0 generator: no estimate
+        M[0, 0, 0] = M[1, 1, 0] = 1
+        rr.analyze_pm_basis(M, np.zeros(2 * b, np.int64), 3323)
+    assert e.value.status == 7
