@@ -1006,26 +1006,65 @@ struct HostCsr {
   int64_t rows = 0, cols = 0;
 };
 
+// Indices by decreasing degree, ties in index order (a stable sort), by a
+// counting sort over the degrees.
 std::vector<int32_t> degree_order(const std::vector<int64_t>& deg) {
-  std::vector<int32_t> order(deg.size());
-  std::iota(order.begin(), order.end(), 0);
-  std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return deg[a] > deg[b]; });
+  const int64_t n = (int64_t)deg.size();
+  int64_t maxd = 0;
+  for (int64_t d : deg) maxd = std::max(maxd, d);
+  std::vector<int64_t> start(maxd + 2, 0);  // bucket maxd - d holds degree d
+  for (int64_t d : deg) start[maxd - d + 1]++;
+  for (int64_t b = 0; b <= maxd; ++b) start[b + 1] += start[b];
+  std::vector<int32_t> order(n);
+  for (int64_t i = 0; i < n; ++i) order[start[maxd - deg[i]]++] = (int32_t)i;
   return order;
 }
 
+// CSR of the transpose, stable by row (entries of a column in increasing row
+// order), on the host's cores: blocks of rows count their columns, each
+// (block, column) pair gets its own output range, and the blocks scatter in
+// parallel.
 void transpose_host(const HostCsr& a, HostCsr& t) {
   t.rows = a.cols;
   t.cols = a.rows;
   t.ptr.assign(a.cols + 1, 0);
-  for (const uint2& e : a.cv) t.ptr[e.x + 1]++;
-  for (int64_t i = 0; i < a.cols; ++i) t.ptr[i + 1] += t.ptr[i];
-  std::vector<uint32_t> next(t.ptr.begin(), t.ptr.end() - 1);
   t.cv.resize(a.cv.size());
-  for (int64_t r = 0; r < a.rows; ++r)
-    for (uint32_t k = a.ptr[r]; k < a.ptr[r + 1]; ++k) {
-      const uint32_t pos = next[a.cv[k].x]++;
-      t.cv[pos] = make_uint2((uint32_t)r, a.cv[k].y);
+  const int64_t hw = std::max(1u, std::thread::hardware_concurrency());
+  // at most 2^26 counters in all
+  const int64_t nblk =
+      std::max<int64_t>(1, std::min<int64_t>({hw, a.rows / 4096, ((int64_t)1 << 26) / std::max<int64_t>(a.cols, 1)}));
+  std::vector<uint32_t> cnt((size_t)nblk * a.cols, 0);
+  auto rlo = [&](int64_t b) { return a.rows * b / nblk; };
+  host_parallel_ranges(nblk, 1, [&](int64_t b0, int64_t b1) {
+    for (int64_t b = b0; b < b1; ++b) {
+      uint32_t* c = cnt.data() + (size_t)b * a.cols;
+      for (uint32_t k = a.ptr[rlo(b)]; k < a.ptr[rlo(b + 1)]; ++k) c[a.cv[k].x]++;
     }
+  });
+  for (int64_t b = 0; b < nblk; ++b) {
+    const uint32_t* c = cnt.data() + (size_t)b * a.cols;
+    for (int64_t i = 0; i < a.cols; ++i) t.ptr[i + 1] += c[i];
+  }
+  for (int64_t i = 0; i < a.cols; ++i) t.ptr[i + 1] += t.ptr[i];
+  // counts -> first output position of each (block, column)
+  host_parallel_ranges(a.cols, (int64_t)1 << 14, [&](int64_t c0, int64_t c1) {
+    for (int64_t c = c0; c < c1; ++c) {
+      uint32_t run = t.ptr[c];
+      for (int64_t b = 0; b < nblk; ++b) {
+        uint32_t& x = cnt[(size_t)b * a.cols + c];
+        const uint32_t k = x;
+        x = run;
+        run += k;
+      }
+    }
+  });
+  host_parallel_ranges(nblk, 1, [&](int64_t b0, int64_t b1) {
+    for (int64_t b = b0; b < b1; ++b) {
+      uint32_t* next = cnt.data() + (size_t)b * a.cols;
+      for (int64_t r = rlo(b); r < rlo(b + 1); ++r)
+        for (uint32_t k = a.ptr[r]; k < a.ptr[r + 1]; ++k) t.cv[next[a.cv[k].x]++] = make_uint2((uint32_t)r, a.cv[k].y);
+    }
+  });
 }
 
 int upload_csr(const HostCsr& h, DevCsr& d, cudaStream_t s) {
@@ -1087,13 +1126,16 @@ int matrix_build(rr_ctx* ctx, int64_t m, int64_t n, const int64_t* rowptr, const
   A.ptr.resize(m + 1);
   A.cv.resize(nnz);
   A.ptr[0] = 0;
-  for (int64_t rp = 0; rp < m; ++rp) {
-    const int64_t r = mat->rowperm[rp];
-    uint32_t o = A.ptr[rp];
-    for (int64_t k = rowptr[r]; k < rowptr[r + 1]; ++k) A.cv[o++] = make_uint2((uint32_t)inv_col[col[k]], val[k]);
-    std::sort(A.cv.begin() + A.ptr[rp], A.cv.begin() + o, [](const uint2& a, const uint2& b) { return a.x < b.x; });
-    A.ptr[rp + 1] = o;
-  }
+  for (int64_t rp = 0; rp < m; ++rp) A.ptr[rp + 1] = A.ptr[rp] + (uint32_t)rdeg[mat->rowperm[rp]];
+  // rows in their new order, columns renumbered and sorted; rows are independent
+  host_parallel_ranges(m, (int64_t)1 << 12, [&](int64_t lo, int64_t hi) {
+    for (int64_t rp = lo; rp < hi; ++rp) {
+      const int64_t r = mat->rowperm[rp];
+      uint32_t o = A.ptr[rp];
+      for (int64_t k = rowptr[r]; k < rowptr[r + 1]; ++k) A.cv[o++] = make_uint2((uint32_t)inv_col[col[k]], val[k]);
+      std::sort(A.cv.begin() + A.ptr[rp], A.cv.begin() + o, [](const uint2& a, const uint2& b) { return a.x < b.x; });
+    }
+  });
   HostCsr At;
   transpose_host(A, At);
   cudaStream_t s = ctx->stream;
