@@ -174,6 +174,13 @@ def ncu_traffic():
         return {}
 
 
+def bench_config(args, m, n, nnz, world):
+    """The `config` dict of the JSON line; both arms print the same one."""
+    full = args.scale == 1.0 and not args.small
+    return {"workload": WORKLOAD if full else f"{WORKLOAD}_scaled", "m": m, "n": n, "nnz": int(nnz), "b": args.b,
+            "p": P, "parallelism": f"replicas x{world}", "l2_policy": "inputs larger than L2 (working set ~0.7 GB)"}
+
+
 def cpu_baseline(rowptr, col, val, m, n, b, samples):
     """The oracle (CPU restatement of the reference's Krylov worker + consumer) on the same matrix."""
     import oracle
@@ -220,8 +227,7 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32 mod p (u64/u128 accum)",
         "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD if not args.small else WORKLOAD + "_small", "b": args.b, "p": P,
-                   "l2_policy": "inputs larger than L2"},
+        "config": bench_config(args, m, n, rowptr[-1], int(os.environ.get("WORLD_SIZE", "1"))),
         "cpu_baseline": {"value": v, "unit": "GB/s", "cores": threads, "kind": "port",
                          "sample": f"{args.steps} applications of B on the full matrix"},
         "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -465,9 +471,7 @@ def run_engine(args):
         "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32 mod p (u64 lazy accum)", "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD if (args.scale == 1.0 and not args.small) else f"{WORKLOAD}_scaled", "m": m, "n": n,
-                   "nnz": int(rowptr[-1]), "b": b, "p": P, "parallelism": f"replicas x{world}",
-                   "l2_policy": "inputs larger than L2 (working set ~0.7 GB)"},
+        "config": bench_config(args, m, n, rowptr[-1], world),
         "roofline": roof, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
         "matrix_setup_s": setup_s,
     }

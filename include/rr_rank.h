@@ -93,6 +93,21 @@ int rr_krylov_destroy(rr_krylov* kr);
  * *new_len receives the new sequence length. */
 int rr_krylov_advance(rr_krylov* kr, int64_t max_nlen, uint32_t* seq, int64_t seq_stride, int64_t* new_len);
 
+/* rr_krylov_advance with the progress report of src/main.rs:57-85
+ * (report_progress) and the timed checkpoint hook of src/main.rs:186-202: the
+ * terms are computed in chunks of chunk_terms (<= 1: one chunk) and after each
+ * chunk, whose terms are already in seq, fn(user, len, target_len, elapsed_s,
+ * terms_per_s) is called (fn may be NULL); terms_per_s is the rate since the
+ * previous report.  A non-zero return from fn stops after that chunk (the
+ * caller saves its .wdm checkpoint and calls again to continue); *new_len is
+ * the length reached. */
+typedef int (*rr_progress_fn)(void* user, int64_t len, int64_t target_len, double elapsed_s, double terms_per_s);
+int rr_krylov_advance_report(rr_krylov* kr, int64_t max_nlen, uint32_t* seq, int64_t seq_stride,
+                             int64_t chunk_terms, rr_progress_fn fn, void* user, int64_t* new_len);
+/* VectorStream::fill_status (src/vectorstream.rs:7-10): a one-line status of
+ * the stream (terms queued, whether device work is in flight) into buf[cap]. */
+int rr_krylov_fill_status(rr_krylov* kr, char* buf, int64_t cap);
+
 /* Device-resident stepping for benchmarks and pipelines: queue n_apps
  * applications of B (2 terms each) on the context stream without any host
  * synchronisation.  Terms stay in the handle's device sequence buffer. */
@@ -123,26 +138,33 @@ int rr_krylov_launch_count(const rr_krylov* kr, int64_t* count);
  * symmetric b x b sequence seq[b(b+1)/2][seq_stride] (nlen valid terms).
  * d is rounded up to a power of two and must be < nlen.  Outputs (host):
  * M[2b][2b][d+1] and delta[2b], identical to the reference's result computed
- * exactly mod p.  Requires p - 1 divisible by the NTT length used (true for
- * p = 2013265921 = 15*2^27+1 up to d = 2^26). */
+ * exactly mod p.  Products are NTT products mod p when p - 1 is divisible by
+ * the transform length (p = 2013265921 = 15*2^27+1 up to d = 2^26), else
+ * exact integer products over two or three NTT primes combined by CRT and
+ * reduced mod p (src/poly_mat_mul.rs:240-256), up to d = 2^23. */
 int rr_pm_basis(rr_ctx* ctx, const uint32_t* seq, int64_t seq_stride, int32_t b, int64_t nlen, int64_t d,
                 uint32_t p, uint32_t* M, int64_t* delta);
 /* No counterpart in the reference.  PM-basis of a short sequence for callers
- * that cannot allocate device memory: code running while a CUDA stream is
- * being captured into a graph, runtimes that hand all device memory to their
- * own pool allocator, or latency-critical loops where cudaMalloc's implicit
- * synchronisation is not acceptable.  Same result as rr_pm_basis, but every
- * pointer is DEVICE memory owned by the caller: d_seq[b(b+1)/2][seq_stride]
+ * that cannot allocate device memory: runtimes that hand all device memory to
+ * their own pool allocator (a cudaMalloc from inside them would fail or
+ * fragment the pool), and latency-critical loops where cudaMalloc's implicit
+ * device synchronisation is not acceptable.  Same result as rr_pm_basis, but
+ * every pointer is DEVICE memory owned by the caller: d_seq[b(b+1)/2][seq_stride]
  * (nlen valid terms), d_M[2b][2b][d'+1] and d_delta[2b] (d' = d rounded up to a
  * power of two).  Limits: 1 <= b <= 16 and d' <= 32 (RR_EINVAL beyond them).
  * The work is queued on `stream` (a cudaStream_t; NULL = legacy default) and
  * the call returns without waiting; outputs are ready when the stream gets
- * there.  Scratch is one fixed 338,176-byte __device__ array inside the
- * library, present on every GPU that loads it until the process exits; the
- * first call on a device looks up its address (make that first call before
- * any stream capture).  All calls share that array: calls whose work can
- * overlap on the GPU (different streams, different host threads) race and
- * must be serialised by the caller. */
+ * there.  A device-side failure cannot be returned by this asynchronous call:
+ * it leaves every d_delta entry at INT64_MIN (exact arithmetic rules it out;
+ * it would mean a fault in the library).  Scratch is one fixed 338,176-byte
+ * __device__ array inside the library, present on every GPU that loads it
+ * until the process exits; the first call on a device looks up its address
+ * and sets a kernel attribute (make that first call before any stream
+ * capture; after cudaDeviceReset the looked-up address is stale and the entry
+ * point must not be called again in that process).  All calls share that
+ * array and it keeps the last call's contents: calls whose work can overlap
+ * on the GPU (different streams, different host threads) race and must be
+ * serialised by the caller. */
 int rr_pm_basis_short_noalloc(const uint32_t* d_seq, int64_t seq_stride, int32_t b, int64_t nlen, int64_t d,
                               uint32_t p, uint32_t* d_M, int64_t* d_delta, void* stream);
 /* analyze_pm_basis + analyze_min_generators (src/sigma_basis.rs:71-152,

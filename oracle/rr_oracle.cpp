@@ -33,7 +33,11 @@ typedef unsigned __int128 u128;
 
 namespace {
 
-inline u64 mulmod(u64 a, u64 b, u64 p) { return (u64)((u128)a * b % p); }
+inline u64 mulmod(u64 a, u64 b, u64 p) {
+  // residues are < 2^31, so the product fits in 64 bits (one 64-bit division)
+  if ((a | b) < (1ull << 32)) return a * b % p;
+  return (u64)((u128)a * b % p);
+}
 inline u64 addmod(u64 a, u64 b, u64 p) { u64 s = a + b; return s >= p ? s - p : s; }
 inline u64 submod(u64 a, u64 b, u64 p) { return a >= b ? a - b : a + p - b; }
 
@@ -159,7 +163,7 @@ void lsp_decomposition(const Mat& in, u64 p, Mat& L, Mat& S, std::vector<int>& p
       L(i, k) = f;
       for (int col = rank; col < m; ++col) {
         const u64 sub = mulmod(f, a(k, col), p);
-        a(i, col) = (a(i, col) + p - sub) % p;
+        a(i, col) = submod(a(i, col) % p, sub, p);
       }
     }
     ++rank;
@@ -195,7 +199,7 @@ bool matrix_inverse(const Mat& m_in, u64 p, Mat& out) {
       const u64 f = aug(j, i);
       for (int k = 0; k < 2 * n; ++k) {
         const u64 t = mulmod(aug(i, k), f, p);
-        aug(j, k) = (aug(j, k) + p - t) % p;
+        aug(j, k) = submod(aug(j, k), t, p);
       }
     }
   }
@@ -224,7 +228,7 @@ i64 modular_rank(Mat mat, u64 p) {
       if (!f) continue;
       for (int j = col; j < nc; ++j) {
         const u64 sub = mulmod(f, mat(rank, j), p);
-        mat(row, j) = (mat(row, j) + p - sub) % p;
+        mat(row, j) = submod(mat(row, j), sub, p);
       }
     }
     ++rank;
@@ -295,11 +299,53 @@ void ntt(u64* a, i64 n, bool invert, u64 p, u64 g) {
   }
 }
 
+// Product modulo the NTT prime q (q - 1 divisible by L): out[i][j][0..lres).
+// Inputs are reduced mod q first (they are residues mod p, p < 2^31).
+void ntt_matmul(const PolyMat& A, const PolyMat& B, i64 b_start, i64 lb, i64 L, u64 q, std::vector<u64>& out) {
+  const int m = A.rows, n = A.cols, k = B.cols;
+  const i64 la = A.len, lres = la + lb - 1;
+  const u64 g = find_generator(q);
+  std::vector<u64> fa((size_t)m * n * L, 0), fb((size_t)n * k * L, 0);
+  out.assign((size_t)m * k * lres, 0);
+#pragma omp parallel for collapse(2)
+  for (int i = 0; i < m; ++i)
+    for (int j = 0; j < n; ++j) {
+      u64* d = &fa[((size_t)i * n + j) * L];
+      for (i64 t = 0; t < la; ++t) d[t] = A.at(i, j)[t] % q;
+      ntt(d, L, false, q, g);
+    }
+#pragma omp parallel for collapse(2)
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < k; ++j) {
+      u64* d = &fb[((size_t)i * k + j) * L];
+      for (i64 t = 0; t < lb; ++t) d[t] = B.at(i, j)[b_start + t] % q;
+      ntt(d, L, false, q, g);
+    }
+#pragma omp parallel for collapse(2)
+  for (int i = 0; i < m; ++i)
+    for (int j = 0; j < k; ++j) {
+      // lazy sums: three products (< 3 q^2 < 2^64 - q) between reductions
+      std::vector<u64> d(L, 0);
+      for (int r = 0; r < n; ++r) {
+        const u64* x = &fa[((size_t)i * n + r) * L];
+        const u64* y = &fb[((size_t)r * k + j) * L];
+        for (i64 l = 0; l < L; ++l) d[l] += x[l] * y[l];
+        if (r % 3 == 2 || r == n - 1)
+          for (i64 l = 0; l < L; ++l) d[l] %= q;
+      }
+      ntt(d.data(), L, true, q, g);
+      std::memcpy(&out[((size_t)i * k + j) * lres], d.data(), sizeof(u64) * lres);
+    }
+}
+
 // src/poly_mat_mul.rs:89-101, 113-256: C = A * B where only coefficients
 // [b_start, b_end) of B take part; output length la + nlenb - 1, reduced mod p.
-// The reference multiplies exactly over a large NTT prime and then reduces;
-// here the product is computed directly mod p (NTT when p is NTT-friendly for
-// the padded length, schoolbook otherwise), which is the same value mod p.
+// The reference multiplies exactly over a large NTT prime and then reduces
+// (src/poly_mat_mul.rs:240-256 over the prime of src/ntt.rs:60-75).  Here:
+// directly mod p when p is NTT-friendly for the padded length; otherwise the
+// exact integer product by CRT over three NTT primes (their product, ~2^92.9,
+// exceeds inner dimension x length x (p-1)^2 for every size used here), reduced
+// mod p; schoolbook for short products.  All give the same value mod p.
 PolyMat poly_mat_mul_red(const PolyMat& A, const PolyMat& B, u64 p, i64 b_start, i64 b_end) {
   const int m = A.rows, n = A.cols, k = B.cols;
   const i64 la = A.len;
@@ -308,36 +354,25 @@ PolyMat poly_mat_mul_red(const PolyMat& A, const PolyMat& B, u64 p, i64 b_start,
   PolyMat C(m, k, lres);
   i64 L = 1;
   while (L < lres) L <<= 1;
-  const bool use_ntt = ((p - 1) % (u64)L == 0) && lres > 32;
-  if (use_ntt) {
-    const u64 g = find_generator(p);
-    std::vector<u64> fa((size_t)m * n * L, 0), fb((size_t)n * k * L, 0), fc((size_t)m * k * L, 0);
-#pragma omp parallel for collapse(2)
-    for (int i = 0; i < m; ++i)
-      for (int j = 0; j < n; ++j) {
-        u64* d = &fa[((size_t)i * n + j) * L];
-        std::memcpy(d, A.at(i, j), sizeof(u64) * la);
-        ntt(d, L, false, p, g);
-      }
-#pragma omp parallel for collapse(2)
-    for (int i = 0; i < n; ++i)
-      for (int j = 0; j < k; ++j) {
-        u64* d = &fb[((size_t)i * k + j) * L];
-        std::memcpy(d, B.at(i, j) + b_start, sizeof(u64) * lb);
-        ntt(d, L, false, p, g);
-      }
-#pragma omp parallel for collapse(2)
-    for (int i = 0; i < m; ++i)
-      for (int j = 0; j < k; ++j) {
-        u64* d = &fc[((size_t)i * k + j) * L];
-        for (int r = 0; r < n; ++r) {
-          const u64* x = &fa[((size_t)i * n + r) * L];
-          const u64* y = &fb[((size_t)r * k + j) * L];
-          for (i64 l = 0; l < L; ++l) d[l] = addmod(d[l], mulmod(x[l], y[l], p), p);
-        }
-        ntt(d, L, true, p, g);
-        std::memcpy(C.at(i, j), d, sizeof(u64) * lres);
-      }
+  if (lres > 32 && (p - 1) % (u64)L == 0) {
+    std::vector<u64> out;
+    ntt_matmul(A, B, b_start, lb, L, p, out);
+    C.a = std::move(out);
+  } else if (lres > 32) {
+    static const u64 Q[3] = {2013265921ull, 2113929217ull, 2130706433ull};
+    std::vector<u64> r[3];
+    for (int i = 0; i < 3; ++i) ntt_matmul(A, B, b_start, lb, L, Q[i], r[i]);
+    const u128 q01 = (u128)Q[0] * Q[1];
+    const u64 c01 = invmod(Q[0] % Q[1], Q[1]), c02 = invmod(Q[0] % Q[2], Q[2]), c12 = invmod(Q[1] % Q[2], Q[2]);
+#pragma omp parallel for
+    for (i64 t = 0; t < (i64)C.a.size(); ++t) {
+      const u64 x0 = r[0][t];
+      const u64 x1 = mulmod(submod(r[1][t], x0 % Q[1], Q[1]), c01, Q[1]);
+      const u64 t2 = mulmod(submod(r[2][t], x0 % Q[2], Q[2]), c02, Q[2]);
+      const u64 x2 = mulmod(submod(t2, x1 % Q[2], Q[2]), c12, Q[2]);
+      const u128 v = (u128)x0 + (u128)x1 * Q[0] + (u128)x2 * q01;
+      C.a[t] = (u64)(v % p);
+    }
   } else {
 #pragma omp parallel for collapse(2)
     for (int i = 0; i < m; ++i)

@@ -17,12 +17,14 @@ from __future__ import annotations
 
 import atexit
 import ctypes as C
+import sys
 import time
 import weakref
 from dataclasses import dataclass
 
 import numpy as np
 
+from . import _lib
 from ._lib import RRError, check, lib, ptr  # noqa: F401
 
 # Live handles by teardown order (states and batches, then matrices, then
@@ -191,7 +193,10 @@ class KrylovStream:
         return list(self.get_curv())
 
     def fill_status(self) -> str:
-        return "device"
+        """src/vectorstream.rs:7-10: one line on the stream's state."""
+        buf = C.create_string_buffer(256)
+        check(lib().rr_krylov_fill_status(self.handle, buf, 256))
+        return buf.value.decode()
 
     def get_curv(self, out: np.ndarray | None = None) -> np.ndarray:
         """The current block w_k, [b][n] in the caller's column order.  `out`: a
@@ -203,9 +208,31 @@ class KrylovStream:
         check(lib().rr_krylov_get_curv(self.handle, ptr(out)))
         return out
 
-    def advance(self, max_nlen: int, seq: np.ndarray) -> int:
+    def advance(self, max_nlen: int, seq: np.ndarray, report=None, chunk_terms: int = 0) -> int:
+        """Extend the sequence up to max_nlen terms (see rr_krylov_advance).
+
+        ``report(len, target_len, elapsed_s, terms_per_s) -> bool`` (optional)
+        is called after every chunk of ``chunk_terms`` terms, like the
+        reference's report_progress (src/main.rs:57-85); returning True stops
+        the advance there (to save a checkpoint, src/main.rs:186-202)."""
         new_len = C.c_int64()
-        check(lib().rr_krylov_advance(self.handle, int(max_nlen), ptr(seq), seq.shape[1], C.byref(new_len)))
+        if report is None:
+            check(lib().rr_krylov_advance(self.handle, int(max_nlen), ptr(seq), seq.shape[1], C.byref(new_len)))
+            return new_len.value
+        errors = []
+
+        def cb(_user, length, target, elapsed, rate):
+            try:
+                return 1 if report(int(length), int(target), float(elapsed), float(rate)) else 0
+            except Exception as e:  # stop and re-raise on the Python side
+                errors.append(e)
+                return 1
+
+        fn = _lib.PROGRESS_FN(cb)
+        check(lib().rr_krylov_advance_report(self.handle, int(max_nlen), ptr(seq), seq.shape[1], int(chunk_terms), fn,
+                                             None, C.byref(new_len)))
+        if errors:
+            raise errors[0]
         return new_len.value
 
     def step_device(self, n_apps: int):
@@ -255,29 +282,45 @@ def default_max_nlen(m: int, n: int, num_v: int) -> int:
     return max_nlen
 
 
+def report_progress(length: int, target: int, elapsed: float, rate: float, num_v: int, out=None) -> None:
+    """The progress line of src/main.rs:57-85: terms done, elapsed time, throughput, time remaining."""
+    remaining = (target - length) / rate if rate > 0 else float("inf")
+    print(f"\rProgress: {length}/{target} | Elapsed: {int(elapsed)}s | Throughput: {rate:.1f}/s "
+          f"(total {rate * num_v:.1f}/s) | Remaining: {remaining:.1f}s", end="", flush=True, file=out or sys.stdout)
+
+
 def main_loop_s_mt2(stream: KrylovStream, row_precond, col_precond, curv, v, seq: np.ndarray, seq_len: int,
                     max_nlen: int, wdm_filename: str | None = None, theprime: int = DEFAULT_PRIME,
-                    save_after: float = 200.0, chunk_terms: int = 1 << 14) -> int:
+                    save_after: float = 200.0, chunk_terms: int = 1 << 14, report_every: float | None = None) -> int:
     """src/main.rs:88-216.  ``seq`` is [b(b+1)/2][>= max_nlen + 1] and holds
     ``seq_len`` terms; returns the new length.  The current block is written
-    back into ``curv`` and, every ``save_after`` seconds, saved to the .wdm file."""
+    back into ``curv`` and, every ``save_after`` seconds, saved to the .wdm
+    file (src/main.rs:186-202); with ``report_every`` (seconds) a progress line
+    is printed like the reference's report_progress (src/main.rs:57-85)."""
     last_save = time.time()
+    last_report = [0.0]
+    b = stream.b
+
+    def report(length, target, elapsed, rate):
+        if report_every is not None and elapsed - last_report[0] >= report_every:
+            report_progress(length, target, elapsed, rate, b)
+            last_report[0] = elapsed
+        # stop the advance when a checkpoint is due
+        return bool(wdm_filename) and time.time() - last_save > save_after
+
     L = seq_len
-    remaining = max(0, (max_nlen - L) // 2)  # applications of B still to run (src/main.rs:109,131)
-    chunk = max(1, chunk_terms // 2)
     while True:
-        k = min(remaining, chunk)
-        # a fresh start also emits S_0 (src/main.rs:113-128)
-        L = stream.advance(L + 2 * k if L > 0 else 2 * k, seq)
-        remaining -= k
-        done = remaining == 0
-        if wdm_filename and (done or time.time() - last_save > save_after):
+        L = stream.advance(max_nlen, seq, report=report, chunk_terms=chunk_terms)
+        done = max_nlen - L < 2
+        if wdm_filename:
             curv[:] = stream.get_curv()
             save_wdm_file_sym(wdm_filename, stream.a.n_rows, stream.n, theprime, row_precond, col_precond, v, curv,
                               seq[:, :L])
             last_save = time.time()
         if done:
             break
+    if report_every is not None:
+        print(file=sys.stdout)
     curv[:] = stream.get_curv()
     return L
 

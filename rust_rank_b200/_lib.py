@@ -21,6 +21,8 @@ STATUS_NAMES = {0: "RR_OK", 1: "RR_EINVAL", 2: "RR_EPRIME", 3: "RR_ENOMEM", 4: "
 _vp = C.c_void_p
 _i32, _i64, _u32 = C.c_int32, C.c_int64, C.c_uint32
 _pi64, _pu32, _pi32 = C.POINTER(C.c_int64), C.POINTER(C.c_uint32), C.POINTER(C.c_int32)
+# rr_progress_fn: int (*)(void* user, int64_t len, int64_t target_len, double elapsed_s, double terms_per_s)
+PROGRESS_FN = C.CFUNCTYPE(C.c_int, _vp, _i64, _i64, C.c_double, C.c_double)
 SIGNATURES = {
     "rr_status_string": (C.c_char_p, [C.c_int]),
     "rr_last_error": (C.c_char_p, []),
@@ -37,6 +39,8 @@ SIGNATURES = {
     "rr_krylov_create": (C.c_int, [_vp, _i32, _vp, _vp, _vp, _i64, C.POINTER(_vp)]),
     "rr_krylov_destroy": (C.c_int, [_vp]),
     "rr_krylov_advance": (C.c_int, [_vp, _i64, _vp, _i64, _pi64]),
+    "rr_krylov_advance_report": (C.c_int, [_vp, _i64, _vp, _i64, _i64, PROGRESS_FN, _vp, _pi64]),
+    "rr_krylov_fill_status": (C.c_int, [_vp, C.c_char_p, _i64]),
     "rr_krylov_step_device": (C.c_int, [_vp, _i64]),
     "rr_krylov_fetch": (C.c_int, [_vp, _i64, _i64, _vp, _i64]),
     "rr_krylov_length": (C.c_int, [_vp, _pi64]),

@@ -1,6 +1,7 @@
 // api.cu -- the C ABI (include/rr_rank.h): contexts, matrices, Krylov handles,
 // generator and rank entry points.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -410,7 +411,8 @@ int rr_krylov_fetch(rr_krylov* kr, int64_t from, int64_t to, uint32_t* seq, int6
   return RR_OK;
 }
 
-int rr_krylov_advance(rr_krylov* kr, int64_t max_nlen, uint32_t* seq, int64_t seq_stride, int64_t* new_len) {
+int rr_krylov_advance_report(rr_krylov* kr, int64_t max_nlen, uint32_t* seq, int64_t seq_stride,
+                             int64_t chunk_terms, rr_progress_fn fn, void* user, int64_t* new_len) {
   if (!kr || !seq || !new_len) return fail(RR_EINVAL, "NULL argument");
   RR_CUDA(cudaSetDevice(kr->mat->ctx->device));
   const int64_t L0 = kr->len;
@@ -421,9 +423,47 @@ int rr_krylov_advance(rr_krylov* kr, int64_t max_nlen, uint32_t* seq, int64_t se
   }
   const int64_t final_len = (L0 == 0 ? 1 : L0) + 2 * (to_be_produced / 2);
   if (seq_stride < final_len) return fail(RR_EINVAL, "seq_stride %lld < %lld terms", (long long)seq_stride, (long long)final_len);
-  RR_TRY(queue_apps(kr, to_be_produced / 2));
-  RR_TRY(rr_krylov_fetch(kr, L0, kr->len, seq, seq_stride));
+  const int64_t apps = to_be_produced / 2;
+  const int64_t chunk = chunk_terms > 1 ? chunk_terms / 2 : std::max<int64_t>(apps, 1);
+  using clk = std::chrono::steady_clock;
+  const auto t0 = clk::now();
+  auto t_last = t0;
+  int64_t fetched = L0, done = 0, len_last = L0;
+  do {
+    const int64_t k = std::min(chunk, apps - done);
+    RR_TRY(queue_apps(kr, k));
+    RR_TRY(rr_krylov_fetch(kr, fetched, kr->len, seq, seq_stride));  // waits for the chunk
+    fetched = kr->len;
+    done += k;
+    if (fn) {  // report_progress (src/main.rs:57-85)
+      const auto now = clk::now();
+      const double dt = std::chrono::duration<double>(now - t_last).count();
+      const double rate = dt > 0 ? (double)(kr->len - len_last) / dt : 0.0;
+      t_last = now;
+      len_last = kr->len;
+      if (fn(user, kr->len, final_len, std::chrono::duration<double>(now - t0).count(), rate) != 0) break;
+    }
+  } while (done < apps);
   *new_len = kr->len;
+  return RR_OK;
+}
+
+int rr_krylov_advance(rr_krylov* kr, int64_t max_nlen, uint32_t* seq, int64_t seq_stride, int64_t* new_len) {
+  return rr_krylov_advance_report(kr, max_nlen, seq, seq_stride, 0, nullptr, nullptr, new_len);
+}
+
+int rr_krylov_fill_status(rr_krylov* kr, char* buf, int64_t cap) {
+  if (!kr || !buf || cap < 1) return fail(RR_EINVAL, "bad argument");
+  RR_CUDA(cudaSetDevice(kr->mat->ctx->device));
+  // terms queued on the context's stream and how many of them have finished
+  int64_t finished = kr->len;
+  const cudaError_t q = cudaStreamQuery(kr->mat->ctx->stream);
+  if (q == cudaErrorNotReady) finished = -1;
+  else if (q != cudaSuccess) RR_CUDA(q);
+  if (finished < 0)
+    snprintf(buf, (size_t)cap, "%lld terms queued on the device, work in flight", (long long)kr->len);
+  else
+    snprintf(buf, (size_t)cap, "%lld terms computed, device idle", (long long)kr->len);
   return RR_OK;
 }
 

@@ -136,8 +136,12 @@ __global__ void __launch_bounds__(512) ntt_fwd_smem_kernel(uint32_t* a, int64_t 
     const int64_t blk = blk0 + g;
     uint32_t v = 0;
     if (blk < nblocks) {
-      if (src.p) v = t < src_len ? src.at(blk)[t] : 0u;  // N == T: block = polynomial
-      else v = a[(blk << logT) + t];
+      if (src.p) {  // N == T: block = polynomial; residues mod p < 2^31 < 2q, one subtraction reduces them mod q
+        v = t < src_len ? src.at(blk)[t] : 0u;
+        v = v >= p ? v - p : v;
+      } else {
+        v = a[(blk << logT) + t];
+      }
     }
     s[e] = v;
   }
@@ -206,12 +210,14 @@ __global__ void __launch_bounds__(512) ntt_inv_smem_kernel(uint32_t* a, int64_t 
   }
 }
 
-// Copy poly q of a strided source into a dense N-length slot with zero padding.
-__global__ void pad_copy_kernel(uint32_t* a, int64_t N, int64_t npoly, PolyView src, int64_t src_len) {
+// Copy poly q of a strided source into a dense N-length slot with zero
+// padding, reduced modulo the transform prime qp (sources are < 2^31 < 2 qp).
+__global__ void pad_copy_kernel(uint32_t* a, int64_t N, int64_t npoly, PolyView src, int64_t src_len, uint32_t qp) {
   const int64_t total = npoly * N;
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
     const int64_t q = t / N, k = t % N;
-    a[t] = (k < src_len) ? src.at(q)[k] : 0u;
+    const uint32_t v = (k < src_len) ? src.at(q)[k] : 0u;
+    a[t] = v >= qp ? v - qp : v;
   }
 }
 
@@ -221,6 +227,43 @@ __global__ void extract_scale_kernel(const uint32_t* a, int64_t N, int64_t npoly
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
     const int64_t q = t / cnt, k = t % cnt;
     dst.at(q)[k] = mul_shoup(a[q * N + lo + k], ninv, ninv_s, p);
+  }
+}
+
+// Exact integer products for primes without a suitable NTT: the product is
+// computed modulo two or three NTT primes q0 < q1 < q2 whose product exceeds
+// every coefficient of the exact integer product (inner dimension x length x
+// (p-1)^2), the residues are combined by Garner's mixed-radix CRT
+//   V = x0 + q0 x1 + q0 q1 x2,  x0 = r0,  x1 = (r1 - x0) q0^-1 mod q1,
+//   x2 = ((r2 - x0) q0^-1 - x1) q1^-1 mod q2,
+// and V is reduced mod p -- the reference's exact-integer-then-reduce
+// semantics (src/poly_mat_mul.rs:240-256 over the prime of src/ntt.rs:60-75).
+struct CrtParams {
+  int k;                  // primes used (2 or 3)
+  uint32_t q[3];
+  ModP Mq[3];
+  uint32_t c01, c02, c12;  // q0^-1 mod q1, q0^-1 mod q2, q1^-1 mod q2
+  uint32_t q0p, q01p;      // q0 mod p, q0 q1 mod p
+  ModP Mp;
+};
+
+__global__ void crt_kernel(const uint32_t* __restrict__ R0, const uint32_t* __restrict__ R1,
+                           const uint32_t* __restrict__ R2, int64_t npoly, int64_t cnt, PolyView dst, CrtParams C) {
+  const int64_t total = npoly * cnt;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t q = t / cnt, j = t - q * cnt;
+    const uint32_t x0 = R0[t];
+    const uint32_t x0m1 = x0 >= C.q[1] ? x0 - C.q[1] : x0;
+    const uint32_t x1 = mulmod(submod(R1[t], x0m1, C.q[1]), C.c01, C.Mq[1]);
+    uint64_t v = (uint64_t)x0 + (uint64_t)x1 * C.q0p;
+    if (C.k == 3) {
+      const uint32_t x0m2 = x0 >= C.q[2] ? x0 - C.q[2] : x0;
+      const uint32_t x1m2 = x1 >= C.q[2] ? x1 - C.q[2] : x1;
+      const uint32_t t2 = mulmod(submod(R2[t], x0m2, C.q[2]), C.c02, C.Mq[2]);
+      const uint32_t x2 = mulmod(submod(t2, x1m2, C.q[2]), C.c12, C.Mq[2]);
+      v += (uint64_t)x2 * C.q01p;  // < 2^31 + 2 * 2^62
+    }
+    dst.at(q)[j] = reduce(v, C.Mp);
   }
 }
 
@@ -577,8 +620,11 @@ __global__ void __launch_bounds__(kBaseThreads) pm_base_kernel(BaseParams P) {
   }
   // normalise rows by sigma^{-1} and write out [i][j][t]
   for (int i = tid; i < m; i += nt) sig_tmp[i] = inv_fermat(sigma[i], M);
-  for (int i = tid; i < m; i += nt) P.delta[i] = sdelta[i];
-  __syncthreads();
+  __syncthreads();  // every status write of this CTA is visible after the barrier
+  // a zero row scale cannot be returned by the asynchronous caller: it marks
+  // the output instead, every delta entry INT64_MIN
+  const bool failed = *(volatile int*)P.status != 0;
+  for (int i = tid; i < m; i += nt) P.delta[i] = failed ? INT64_MIN : sdelta[i];
   for (int e = tid; e < (K + 1) * m * m; e += nt) {
     const int t = e / (m * m), i = (e / m) % m, c = e % m;
     P.Mout[(int64_t)i * P.out_rs + (int64_t)c * P.out_cs + t] = mulmod(Mc[e], sig_tmp[i], M);
@@ -1424,6 +1470,31 @@ int grid_for(int64_t work, int threads = 256) {
   return (int)std::max<int64_t>(1, std::min<int64_t>(b, 148 * 32));
 }
 
+// An NTT prime q with its twiddle tables (w^j and Shoup quotients, forward
+// and inverse, j < nmax / 2) and the pointwise stage's fold rule.
+struct NttPrime {
+  uint32_t q = 0;
+  ModP M{};
+  int fold4 = 0;
+  int64_t nmax = 0;
+  DevBuf<uint32_t> tw, tws, twi, twis;
+  Twiddles fwd() const { return Twiddles{tw.ptr, tws.ptr, nmax}; }
+  Twiddles inv() const { return Twiddles{twi.ptr, twis.ptr, nmax}; }
+};
+
+// Four products fit between folds of a 64-bit accumulator iff
+// (2^32 - 1) * c32 + 2^32 - 1 + 4 (q - 1)^2 < 2^64.
+int fold4_ok(uint32_t q, const ModP& M) {
+  const unsigned __int128 F = (unsigned __int128)0xffffffffull * M.c32 + 0xffffffffull;
+  const unsigned __int128 sq = (unsigned __int128)(q - 1) * (q - 1);
+  return (F + 4 * sq) < ((unsigned __int128)1 << 64);
+}
+
+// The three largest NTT primes below 2^31 (2-adic orders 27, 25, 24): the
+// exact-integer products of primes without a suitable NTT are taken modulo
+// the first two or three of them.
+constexpr uint32_t kCrtPrimes[3] = {2013265921u, 2113929217u, 2130706433u};
+
 struct Pm {
   rr_ctx* ctx = nullptr;
   cudaStream_t s = nullptr;
@@ -1434,7 +1505,11 @@ struct Pm {
   int K = 0;
   bool use_ntt = false;
   int64_t nmax = 0;
-  DevBuf<uint32_t> tw, tws, twi, twis;
+  // transform primes: {p} when p - 1 is divisible by nmax, else two or three
+  // of kCrtPrimes with the products combined by CRT
+  std::vector<std::unique_ptr<NttPrime>> nps;
+  bool crt = false;
+  DevBuf<uint32_t> R[3];                // CRT residues [nb][m*m][d+1] per prime
   DevBuf<uint32_t> FA, FB, FC;          // [nb][m*m][nmax]
   DevBuf<uint32_t> Tt;                  // leaf transforms of one block [nb][K][m][m]
   DevBuf<unsigned long long> leafmask;  // [nb][K]
@@ -1446,8 +1521,6 @@ struct Pm {
   bool mma = false;                    // tensor-core leaves kernel (b <= 16)
   // per recursion depth: MM, GG, MMM ([nb] each)
   std::vector<std::unique_ptr<DevBuf<uint32_t>>> bufs;
-  Twiddles fwd() const { return Twiddles{tw.ptr, tws.ptr, nmax}; }
-  Twiddles inv() const { return Twiddles{twi.ptr, twis.ptr, nmax}; }
 };
 
 // A strided polynomial matrix of every generator of the batch: entry (i, j)
@@ -1477,54 +1550,87 @@ NttShape ntt_shape(int64_t T, int64_t nblocks) {
   return sh;
 }
 
-int ntt_forward(Pm& P, uint32_t* a, int64_t N, PolyView src, int64_t src_len) {
+int ntt_forward(Pm& P, const NttPrime& Q, uint32_t* a, int64_t N, PolyView src, int64_t src_len) {
   const int64_t npoly = (int64_t)P.nb * src.npb;
   const int64_t T = std::min<int64_t>(N, kNttBlock);
   if (N <= kNttBlock) {
     const NttShape sh = ntt_shape(T, npoly);
-    ntt_fwd_smem_kernel<<<sh.grid, sh.threads, sh.smem, P.s>>>(a, N, sh.logT, npoly, src, src_len, P.fwd(), P.p);
+    ntt_fwd_smem_kernel<<<sh.grid, sh.threads, sh.smem, P.s>>>(a, N, sh.logT, npoly, src, src_len, Q.fwd(), Q.q);
     RR_CUDA(cudaGetLastError());
     return RR_OK;
   }
-  pad_copy_kernel<<<grid_for(npoly * N), 256, 0, P.s>>>(a, N, npoly, src, src_len);
+  pad_copy_kernel<<<grid_for(npoly * N), 256, 0, P.s>>>(a, N, npoly, src, src_len, Q.q);
   RR_CUDA(cudaGetLastError());
   for (int64_t len = N; len > kNttBlock; len >>= 1) {
-    ntt_fwd_stage_kernel<<<grid_for(npoly * N / 2), 256, 0, P.s>>>(a, N, npoly, len, P.fwd(), P.p);
+    ntt_fwd_stage_kernel<<<grid_for(npoly * N / 2), 256, 0, P.s>>>(a, N, npoly, len, Q.fwd(), Q.q);
     RR_CUDA(cudaGetLastError());
   }
   const PolyView none{nullptr, 1, 1, 0, 0, 0};
   const NttShape sh = ntt_shape(T, npoly * (N / T));
-  ntt_fwd_smem_kernel<<<sh.grid, sh.threads, sh.smem, P.s>>>(a, N, sh.logT, npoly * (N / T), none, 0, P.fwd(), P.p);
+  ntt_fwd_smem_kernel<<<sh.grid, sh.threads, sh.smem, P.s>>>(a, N, sh.logT, npoly * (N / T), none, 0, Q.fwd(), Q.q);
   RR_CUDA(cudaGetLastError());
   return RR_OK;
 }
 
 // Inverse NTTs of a ([nb * npb][N]); coefficients [lo, lo + cnt), scaled by
 // N^{-1}, go to dst.
-int ntt_inverse(Pm& P, uint32_t* a, int64_t N, PolyView dst, int64_t lo, int64_t cnt) {
+int ntt_inverse(Pm& P, const NttPrime& Q, uint32_t* a, int64_t N, PolyView dst, int64_t lo, int64_t cnt) {
   const int64_t npoly = (int64_t)P.nb * dst.npb;
   const int64_t T = std::min<int64_t>(N, kNttBlock);
-  const uint32_t ninv = host_invmod((uint32_t)(N % P.p), P.p);
-  const uint32_t ninv_s = (uint32_t)(((uint64_t)ninv << 32) / P.p);
+  const uint32_t ninv = host_invmod((uint32_t)(N % Q.q), Q.q);
+  const uint32_t ninv_s = (uint32_t)(((uint64_t)ninv << 32) / Q.q);
   if (N <= kNttBlock) {
     const NttShape sh = ntt_shape(T, npoly);
     ntt_inv_smem_kernel<<<sh.grid, sh.threads, sh.smem, P.s>>>(a, N, sh.logT, npoly, dst, lo, cnt, ninv, ninv_s,
-                                                               P.inv(), P.p);
+                                                               Q.inv(), Q.q);
     RR_CUDA(cudaGetLastError());
     return RR_OK;
   }
   const PolyView none{nullptr, 1, 1, 0, 0, 0};
   const NttShape sh = ntt_shape(T, npoly * (N / T));
   ntt_inv_smem_kernel<<<sh.grid, sh.threads, sh.smem, P.s>>>(a, N, sh.logT, npoly * (N / T), none, 0, 0, 0, 0,
-                                                             P.inv(), P.p);
+                                                             Q.inv(), Q.q);
   RR_CUDA(cudaGetLastError());
   for (int64_t len = 2 * kNttBlock; len <= N; len <<= 1) {
-    ntt_inv_stage_kernel<<<grid_for(npoly * N / 2), 256, 0, P.s>>>(a, N, npoly, len, P.inv(), P.p);
+    ntt_inv_stage_kernel<<<grid_for(npoly * N / 2), 256, 0, P.s>>>(a, N, npoly, len, Q.inv(), Q.q);
     RR_CUDA(cudaGetLastError());
   }
-  extract_scale_kernel<<<grid_for(npoly * cnt), 256, 0, P.s>>>(a, N, npoly, dst, lo, cnt, ninv, ninv_s, P.p);
+  extract_scale_kernel<<<grid_for(npoly * cnt), 256, 0, P.s>>>(a, N, npoly, dst, lo, cnt, ninv, ninv_s, Q.q);
   RR_CUDA(cudaGetLastError());
   return RR_OK;
+}
+
+// One NTT product modulo the transform prime Q: coefficients [lo, lo + cnt)
+// of A * B into dst.
+int ntt_product(Pm& P, const NttPrime& Q, MatView A, int mA, int r, int64_t la, MatView B, int k, int64_t lb,
+                int64_t N, PolyView dst, int64_t lo, int64_t cnt) {
+  RR_TRY(ntt_forward(P, Q, P.FA.ptr, N, A.polys(r, mA), la));
+  RR_TRY(ntt_forward(P, Q, P.FB.ptr, N, B.polys(k, r), lb));
+  if (mA % 4 == 0 && k % 4 == 0)
+    pointwise_kernel<<<grid_for((int64_t)P.nb * (mA / 4) * (k / 4) * N), 256, 0, P.s>>>(
+        P.FA.ptr, P.FB.ptr, P.FC.ptr, mA, r, k, N, P.nb, Q.fold4 ? 3 : 1, Q.M);
+  else
+    pointwise1_kernel<<<grid_for((int64_t)P.nb * mA * k * N), 256, 0, P.s>>>(P.FA.ptr, P.FB.ptr, P.FC.ptr, mA, r, k, N,
+                                                                              P.nb, Q.M);
+  RR_CUDA(cudaGetLastError());
+  return ntt_inverse(P, Q, P.FC.ptr, N, dst, lo, cnt);
+}
+
+CrtParams crt_params(const Pm& P) {
+  CrtParams C;
+  C.k = (int)P.nps.size();
+  for (int i = 0; i < 3; ++i) {
+    C.q[i] = i < C.k ? P.nps[i]->q : 1u;
+    C.Mq[i] = i < C.k ? P.nps[i]->M : ModP{};
+  }
+  const uint32_t q0 = C.q[0], q1 = C.q[1];
+  C.c01 = host_invmod(q0 % q1, q1);
+  C.c02 = C.k == 3 ? host_invmod(q0 % C.q[2], C.q[2]) : 0;
+  C.c12 = C.k == 3 ? host_invmod(q1 % C.q[2], C.q[2]) : 0;
+  C.q0p = q0 % P.p;
+  C.q01p = (uint32_t)((uint64_t)(q0 % P.p) * (q1 % P.p) % P.p);
+  C.Mp = P.M;
+  return C;
 }
 
 // dst[i][j][0..cnt) = coefficients [lo, lo+cnt) of A * B for every generator
@@ -1542,16 +1648,18 @@ int poly_mat_mul(Pm& P, MatView A, int mA, int r, int64_t la, MatView B, int k, 
     return RR_OK;
   }
   if (N > P.nmax) return fail(RR_EINVAL, "internal: NTT length %lld exceeds table %lld", (long long)N, (long long)P.nmax);
-  RR_TRY(ntt_forward(P, P.FA.ptr, N, A.polys(r, mA), la));
-  RR_TRY(ntt_forward(P, P.FB.ptr, N, B.polys(k, r), lb));
-  if (mA % 4 == 0 && k % 4 == 0)
-    pointwise_kernel<<<grid_for((int64_t)P.nb * (mA / 4) * (k / 4) * N), 256, 0, P.s>>>(
-        P.FA.ptr, P.FB.ptr, P.FC.ptr, mA, r, k, N, P.nb, P.fold4 ? 3 : 1, P.M);
-  else
-    pointwise1_kernel<<<grid_for((int64_t)P.nb * mA * k * N), 256, 0, P.s>>>(P.FA.ptr, P.FB.ptr, P.FC.ptr, mA, r, k, N,
-                                                                              P.nb, P.M);
+  if (!P.crt) return ntt_product(P, *P.nps[0], A, mA, r, la, B, k, lb, N, dst.polys(k, mA), lo, cnt);
+  // residues per transform prime, dense [nb][mA * k][cnt], then CRT into dst
+  const int64_t per = (int64_t)mA * k * cnt;
+  for (size_t i = 0; i < P.nps.size(); ++i) {
+    const PolyView Rv{P.R[i].ptr, k, mA * k, (int64_t)k * cnt, cnt, per};
+    RR_TRY(ntt_product(P, *P.nps[i], A, mA, r, la, B, k, lb, N, Rv, lo, cnt));
+  }
+  const int64_t npoly = (int64_t)P.nb * mA * k;
+  crt_kernel<<<grid_for(npoly * cnt), 256, 0, P.s>>>(P.R[0].ptr, P.R[1].ptr, P.nps.size() > 2 ? P.R[2].ptr : nullptr,
+                                                     npoly, cnt, dst.polys(k, mA), crt_params(P));
   RR_CUDA(cudaGetLastError());
-  return ntt_inverse(P, P.FC.ptr, N, dst.polys(k, mA), lo, cnt);
+  return RR_OK;
 }
 
 int run_base(Pm& P, MatView G, int nleaves, MatView Mout) {
@@ -1667,6 +1775,7 @@ size_t pm_workspace_bytes(int b, int64_t d) {
   for (int64_t dd = d; dd > 1; dd /= 2) bytes += (2 * m * m + m * n) * (size_t)(dd / 2 + 1) * 4;  // per depth
   bytes += (m * n + m * m) * (size_t)(d + 1) * 4 + (size_t)b * (b + 1) / 2 * (size_t)(d + 1) * 4;  // G, Mo, seq
   bytes += 64 * m * m * 4;                                    // leaf transforms
+  bytes += 3 * m * m * (size_t)(d + 1) * 4;                   // CRT residues (primes without a suitable NTT)
   return bytes;
 }
 
@@ -1687,47 +1796,69 @@ int pm_basis_batch_device(rr_ctx* ctx, int nb, const uint32_t* const* seqs, cons
   P.mma = P.m <= kMmaRows && P.n <= kMmaCols;
   P.K = pick_block_leaves(P.m, P.n, d, P.mma, &leaves_smem);
   P.cs = leaf_coeff_stride(P.m, P.n);
-  {
-    // four products fit between folds iff (2^32-1)*c32 + 2^32 - 1 + 4 (p-1)^2 < 2^64
-    const unsigned __int128 F = (unsigned __int128)0xffffffffull * P.M.c32 + 0xffffffffull;
-    const unsigned __int128 q = (unsigned __int128)(p - 1) * (p - 1);
-    P.fold4 = (F + 4 * q) < ((unsigned __int128)1 << 64);
-  }
+  P.fold4 = fold4_ok(p, P.M);
   const int m = P.m, n = P.n;
   // NTT table for the largest product: length nextpow2(3d/2 + 1) = 2d (d >= 2)
   int64_t nmax = 1;
   while (nmax < d + d / 2 + 1) nmax <<= 1;
   nmax = std::max<int64_t>(nmax, 2);
   P.nmax = nmax;
-  // NTT products need p - 1 divisible by the transform length; other primes
-  // use the direct product (quadratic in the degree)
-  P.use_ntt = d > P.K && (uint64_t)(p - 1) % (uint64_t)nmax == 0;
+  // NTT products: modulo p itself when p - 1 is divisible by the transform
+  // length, else exact integer products by CRT over two or three NTT primes
+  // (whose product must exceed inner dimension x length x (p-1)^2)
+  P.use_ntt = d > P.K;
   if (P.use_ntt) {
-    const uint32_t g = find_generator(p);
-    const uint32_t w = host_powmod(g, (p - 1) / (uint64_t)nmax, p);
-    const uint32_t wi = host_invmod(w, p);
-    std::vector<uint32_t> t(nmax / 2), ts(nmax / 2), ti(nmax / 2), tis(nmax / 2);
-    uint64_t x = 1, y = 1;
-    for (int64_t j = 0; j < nmax / 2; ++j) {
-      t[j] = (uint32_t)x;
-      ti[j] = (uint32_t)y;
-      ts[j] = (uint32_t)((x << 32) / p);
-      tis[j] = (uint32_t)((y << 32) / p);
-      x = x * w % p;
-      y = y * wi % p;
+    std::vector<uint32_t> qs;
+    if ((uint64_t)(p - 1) % (uint64_t)nmax == 0) {
+      qs.push_back(p);
+    } else {
+      P.crt = true;
+      const long double bound = (long double)m * (long double)(d + 1) * (long double)(p - 1) * (long double)(p - 1);
+      long double prod = 1;
+      for (int i = 0; i < 3 && prod <= bound; ++i) {
+        if ((uint64_t)(kCrtPrimes[i] - 1) % (uint64_t)nmax != 0)
+          return fail(RR_EUNSUPPORTED, "d = %lld: NTT length %lld beyond the CRT primes", (long long)d, (long long)nmax);
+        qs.push_back(kCrtPrimes[i]);
+        prod *= kCrtPrimes[i];
+      }
+      if (prod <= bound) return fail(RR_EUNSUPPORTED, "d = %lld too large for a three-prime CRT at p = %u", (long long)d, p);
+      if (qs.size() < 2) qs.push_back(kCrtPrimes[1]);  // Garner needs two residues
     }
-    RR_TRY(P.tw.alloc_async(nmax / 2, P.s));
-    RR_TRY(P.tws.alloc_async(nmax / 2, P.s));
-    RR_TRY(P.twi.alloc_async(nmax / 2, P.s));
-    RR_TRY(P.twis.alloc_async(nmax / 2, P.s));
-    RR_CUDA(cudaMemcpyAsync(P.tw.ptr, t.data(), t.size() * 4, cudaMemcpyHostToDevice, P.s));
-    RR_CUDA(cudaMemcpyAsync(P.tws.ptr, ts.data(), ts.size() * 4, cudaMemcpyHostToDevice, P.s));
-    RR_CUDA(cudaMemcpyAsync(P.twi.ptr, ti.data(), ti.size() * 4, cudaMemcpyHostToDevice, P.s));
-    RR_CUDA(cudaMemcpyAsync(P.twis.ptr, tis.data(), tis.size() * 4, cudaMemcpyHostToDevice, P.s));
+    std::vector<uint32_t> t(nmax / 2), ts(nmax / 2), ti(nmax / 2), tis(nmax / 2);
+    for (uint32_t q : qs) {
+      std::unique_ptr<NttPrime> Q(new NttPrime());
+      Q->q = q;
+      Q->M = make_modp(q);
+      Q->fold4 = fold4_ok(q, Q->M);
+      Q->nmax = nmax;
+      const uint32_t g = find_generator(q);
+      const uint32_t w = host_powmod(g, (q - 1) / (uint64_t)nmax, q);
+      const uint32_t wi = host_invmod(w, q);
+      uint64_t x = 1, y = 1;
+      for (int64_t j = 0; j < nmax / 2; ++j) {
+        t[j] = (uint32_t)x;
+        ti[j] = (uint32_t)y;
+        ts[j] = (uint32_t)((x << 32) / q);
+        tis[j] = (uint32_t)((y << 32) / q);
+        x = x * w % q;
+        y = y * wi % q;
+      }
+      RR_TRY(Q->tw.alloc_async(nmax / 2, P.s));
+      RR_TRY(Q->tws.alloc_async(nmax / 2, P.s));
+      RR_TRY(Q->twi.alloc_async(nmax / 2, P.s));
+      RR_TRY(Q->twis.alloc_async(nmax / 2, P.s));
+      RR_CUDA(cudaMemcpyAsync(Q->tw.ptr, t.data(), t.size() * 4, cudaMemcpyHostToDevice, P.s));
+      RR_CUDA(cudaMemcpyAsync(Q->tws.ptr, ts.data(), ts.size() * 4, cudaMemcpyHostToDevice, P.s));
+      RR_CUDA(cudaMemcpyAsync(Q->twi.ptr, ti.data(), ti.size() * 4, cudaMemcpyHostToDevice, P.s));
+      RR_CUDA(cudaMemcpyAsync(Q->twis.ptr, tis.data(), tis.size() * 4, cudaMemcpyHostToDevice, P.s));
+      RR_CUDA(cudaStreamSynchronize(P.s));  // the host tables are reused for the next prime
+      P.nps.push_back(std::move(Q));
+    }
     RR_TRY(P.FA.alloc_async((size_t)nb * m * m * nmax, P.s));
     RR_TRY(P.FB.alloc_async((size_t)nb * m * m * nmax, P.s));
     RR_TRY(P.FC.alloc_async((size_t)nb * m * m * nmax, P.s));
-    RR_CUDA(cudaStreamSynchronize(P.s));  // the host tables die at scope end
+    if (P.crt)
+      for (size_t i = 0; i < P.nps.size(); ++i) RR_TRY(P.R[i].alloc_async((size_t)nb * m * m * (d + 1), P.s));
   }
   // per-depth buffers
   {
@@ -1789,10 +1920,13 @@ int pm_basis_device(rr_ctx* ctx, const uint32_t* seq, int64_t seq_stride, int b,
 }
 
 // ---------------------------------------------------------------- no-allocation variant
-// rr_pm_basis_short_noalloc runs the same two kernels as rr_pm_basis does for a
-// short sequence (build_G_kernel, then one pm_base_kernel block), but takes its
-// scratch -- the matrix G, the base kernel's double-buffered basis and the
-// status word -- from the file-scope array below instead of allocating it.
+// rr_pm_basis_short_noalloc builds G (build_G_kernel) and runs one block of
+// leaves in one CTA of pm_base_kernel -- the original single-kernel block,
+// kept for this entry point; rr_pm_basis now runs the leaves and the block
+// basis as two kernels.  tests/test_zz_no_alloc.py checks both against each
+// other and against the oracle.  Its scratch -- the matrix G, the base
+// kernel's double-buffered basis and the status word -- comes from the
+// file-scope array below instead of an allocation.
 // Limits: b <= 16 and d (rounded up to a power of two) <= 32.
 namespace {
 constexpr int kNoallocMaxB = 16;
@@ -1815,7 +1949,10 @@ unsigned char* g_noalloc_addr[kNoallocMaxDevices] = {};
 static __device__ __align__(256) unsigned char g_pm_noalloc_scratch[kNoallocScratchBytes];
 
 // Device address of the scratch array on the current device, looked up once
-// per device (host code must not use the symbol itself as an address).
+// per device (host code must not use the symbol itself as an address).  The
+// same first call per device raises pm_base_kernel's shared-memory limit to
+// the largest size this entry point launches, so no later call changes a
+// kernel attribute.
 static int noalloc_scratch(unsigned char** out) {
   int dev = 0;
   RR_CUDA(cudaGetDevice(&dev));
@@ -1824,6 +1961,7 @@ static int noalloc_scratch(unsigned char** out) {
   if (!g_noalloc_addr[dev]) {
     void* p = nullptr;
     RR_CUDA(cudaGetSymbolAddress(&p, g_pm_noalloc_scratch));
+    RR_TRY(set_base_smem_limit(base_smem_bytes(2 * kNoallocMaxB, kNoallocMaxB, kNoallocMaxD, false)));
     g_noalloc_addr[dev] = static_cast<unsigned char*>(p);
   }
   *out = g_noalloc_addr[dev];
@@ -1875,8 +2013,7 @@ extern "C" int rr_pm_basis_short_noalloc(const uint32_t* d_seq, int64_t seq_stri
   B.m_smem = 0;  // the basis stays in the scratch array
   B.M = make_modp(p);
   B.status = status;
-  const size_t bytes = base_smem_bytes(m, n, (int)dd, false);
-  RR_TRY(set_base_smem_limit(bytes));
+  const size_t bytes = base_smem_bytes(m, n, (int)dd, false);  // within the limit set at the first call
   if (n % 4 == 0) pm_base_kernel<4><<<1, kBaseThreads, bytes, s>>>(B);
   else pm_base_kernel<1><<<1, kBaseThreads, bytes, s>>>(B);
   RR_CUDA(cudaGetLastError());

@@ -1,9 +1,10 @@
 """Regenerate the golden fixtures in tests/golden/ from the reference itself.
 
-Run from the repository root in a checkout that has the reference at
-/root/reference (read-only) and the reference harness built:
+Run from the repository root with a wilthoma/rust_rank checkout (read-only)
+and the reference harness built from it:
 
-    make -C oracle && python tests/golden/make_golden.py
+    make -C oracle REF_DIR=<checkout>/cuda_test
+    python tests/golden/make_golden.py --reference <checkout>
 
 Fixtures written (all small):
   matrix_txt.npz      -- the reference's fixture cuda_test/matrix.txt as CSR
@@ -34,7 +35,6 @@ sys.path.insert(0, ROOT)
 import oracle  # noqa: E402
 from rust_rank_b200 import synth  # noqa: E402
 
-REF_FIXTURE = "/root/reference/cuda_test/matrix.txt"
 OUT = os.path.join(ROOT, "tests", "golden")
 P_SMALL = 3323
 
@@ -74,12 +74,18 @@ def ref_pm(R, seq, b, d, p):
 
 
 def main():
+    import argparse
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", required=True, help="root of the wilthoma/rust_rank checkout")
+    args = ap.parse_args()
+    ref_fixture = os.path.join(args.reference, "cuda_test", "matrix.txt")
     R = oracle.ref_lib()
     if R is None:
-        raise SystemExit("oracle/_ref/libref.so missing: run `make -C oracle` with the reference present")
+        raise SystemExit("oracle/_ref/libref.so missing: run `make -C oracle REF_DIR=<checkout>/cuda_test`")
     # --- matrix.txt
-    raw = open(REF_FIXTURE, "rb").read()
-    (m, n), rows, cols, vals = read_sms_signed(REF_FIXTURE)
+    raw = open(ref_fixture, "rb").read()
+    (m, n), rows, cols, vals = read_sms_signed(ref_fixture)
     order = np.argsort(rows, kind="stable")
     rowptr = np.zeros(m + 1, np.int64)
     rowptr[1:] = np.cumsum(np.bincount(rows, minlength=m))

@@ -1,12 +1,12 @@
 """The allocation-free PM-basis entry point (rr_pm_basis_short_noalloc).
 
 Some callers cannot allocate device memory at the moment they need a short
-generator: code that runs while a stream is captured into a CUDA graph, hosts
-whose device memory is owned by their own pool allocator, or loops that cannot
-afford cudaMalloc's implicit synchronisation.  This entry point serves them
-from a fixed scratch array inside the library; its output must equal the
-regular entry point's (rr_pm_basis) exactly, including on back-to-back calls
-that share the scratch array.
+generator: hosts whose device memory is owned by their own pool allocator, or
+loops that cannot afford cudaMalloc's implicit synchronisation.  This entry
+point serves them from a fixed scratch array inside the library; its output
+must equal the regular entry point's (rr_pm_basis) and the oracle's exactly,
+including on back-to-back calls that share the scratch array, and must not
+carry the failure marker (every delta entry INT64_MIN).
 
 Collected last on purpose (file name) so that a stop-at-first-failure run has
 already run every other test when this one runs.
@@ -16,6 +16,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
+import oracle
 import rust_rank_b200 as rr
 from rust_rank_b200 import _lib
 
@@ -50,8 +51,12 @@ def test_matches_regular_entry_point_on_two_calls(b, d, p):
         seq = rng.integers(0, p, size=(b * (b + 1) // 2, dd + 1 + call)).astype(np.uint32)
         M_ref, delta_ref = rr.PM_Basis(seq, d, p)
         M, delta = noalloc_pm_basis(seq, b, d, p)
+        assert not np.all(delta == np.iinfo(np.int64).min), f"call {call}: device-side failure marker"
         assert np.array_equal(M, M_ref), f"call {call}"
         assert np.array_equal(delta, delta_ref), f"call {call}"
+        M_orc, delta_orc = oracle.pm_basis(seq, b, d, p)
+        assert np.array_equal(M, M_orc.astype(np.uint32)), f"call {call}"
+        assert np.array_equal(delta, delta_orc), f"call {call}"
 
 
 def test_rejects_sizes_beyond_the_limit():
