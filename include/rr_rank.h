@@ -271,6 +271,53 @@ int rr_server_stats(rr_server* server, int64_t* submitted, int64_t* completed, d
                     double* ranks_per_s);
 int rr_server_destroy(rr_server* server);
 
+/* ---------------------------------------------------------------- several GPUs */
+/* No counterpart in the reference (it ranks one matrix per run,
+ * src/main.rs:254-639).  Matrices are independent, so the batched and served
+ * modes shard by matrix: each matrix is placed whole on one GPU by its device
+ * footprint and only its rank comes back; no collective, no peer memory. */
+
+/* Device bytes a matrix of this shape and its Krylov state hold while
+ * resident (both CSR copies, blocks, preconditioner forms, sequence of the
+ * length rule of src/main.rs:497-504), the figure admission and placement use. */
+int rr_footprint(int64_t m, int64_t n, int64_t nnz, int32_t b, uint64_t* bytes);
+/* The placement rule (host only): items in decreasing footprint order, each
+ * on the device with the most room left (dev_free[d] minus what it already
+ * got; ties: lowest index).  device_of[nitems] receives device indices into
+ * dev_free; dev_load[ndev] (may be NULL) the bytes placed per device.
+ * RR_ENOMEM when an item fits on no device. */
+int rr_place_by_footprint(int32_t nitems, const uint64_t* footprint, int32_t ndev, const uint64_t* dev_free,
+                          int32_t* device_of, uint64_t* dev_load);
+
+/* One rank service (rr_server_*) per listed device (a device may be listed
+ * more than once: several services share it).  A submitted request goes to
+ * the service with the most budget left after the requests it holds and
+ * follows rr_server's path there, so its rank equals rr_rank's. */
+typedef struct rr_fleet_s rr_fleet;
+int rr_fleet_create(const int32_t* devices, int32_t ndev, const rr_server_config* cfg, rr_fleet** out);
+int rr_fleet_submit(rr_fleet* fleet, int64_t m, int64_t n, const int64_t* rowptr, const int32_t* col,
+                    const uint32_t* val, const uint32_t* row_precond, const uint32_t* col_precond, const uint32_t* V,
+                    uint64_t* id);
+int rr_fleet_wait(rr_fleet* fleet, uint64_t id, double timeout_s, int64_t* rank, double* latency_ms);
+/* The device request id was placed on. */
+int rr_fleet_device_of(rr_fleet* fleet, uint64_t id, int32_t* device);
+/* rr_server_stats over all services: latency percentiles of all completed
+ * requests, completions per second from the first submit to the last completion. */
+int rr_fleet_stats(rr_fleet* fleet, int64_t* submitted, int64_t* completed, double* p50_ms, double* p99_ms,
+                   double* ranks_per_s);
+int rr_fleet_destroy(rr_fleet* fleet);
+
+/* rr_batch_ranks over several devices: the matrices (arguments as for
+ * rr_batch_create) are placed by rr_place_by_footprint on 80% of each
+ * device's free memory (shared evenly by repeated entries), each device runs
+ * one batch of its matrices on a host thread of its own, and ranks[nmat]
+ * come back in the caller's order; device_of[nmat] (may be NULL) receives
+ * the device of each matrix.  Each rank equals rr_rank's on that matrix. */
+int rr_batch_ranks_multi(const int32_t* devices, int32_t ndev, int32_t nmat, const int64_t* m, const int64_t* n,
+                         const int64_t* const* rowptr, const int32_t* const* col, const uint32_t* const* val,
+                         uint32_t p, int32_t b, const uint32_t* const* row_precond, const uint32_t* const* col_precond,
+                         const uint32_t* const* V, int32_t workers, int64_t* ranks, int32_t* device_of);
+
 /* ---------------------------------------------------------------- files */
 /* .wdm checkpoint (src/wdm_files.rs:10-19): header "m n p Nlen num_v", then
  * row_precond, col_precond, num_v lines of v, num_v lines of curv and

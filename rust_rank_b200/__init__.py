@@ -559,6 +559,107 @@ class Server:
             pass
 
 
+def footprint(m: int, n: int, nnz: int, num_v: int) -> int:
+    """Device bytes a matrix and its Krylov state hold while resident (rr_footprint)."""
+    v = C.c_uint64()
+    check(lib().rr_footprint(int(m), int(n), int(nnz), int(num_v), C.byref(v)))
+    return v.value
+
+
+def place_by_footprint(footprints, dev_free):
+    """Placement of independent matrices on devices (rr_place_by_footprint):
+    largest first, each onto the device with the most room left.  Returns
+    (device index per item, bytes placed per device)."""
+    fp = np.ascontiguousarray(footprints, np.uint64)
+    fr = np.ascontiguousarray(dev_free, np.uint64)
+    where = np.zeros(fp.size, np.int32)
+    load = np.zeros(fr.size, np.uint64)
+    check(lib().rr_place_by_footprint(fp.size, ptr(fp), fr.size, ptr(fr), ptr(where), ptr(load)))
+    return where, load
+
+
+def _pointer_arrays(keep, xs, dt):
+    out = [np.ascontiguousarray(x, dt) for x in xs]
+    keep.extend(out)
+    return (C.c_void_p * len(out))(*[a.ctypes.data for a in out])
+
+
+def batch_ranks_multi(mats, num_v: int, theprime: int, row_preconds, col_preconds, vs, devices, workers: int = 8):
+    """Ranks of many matrices over several GPUs (rr_batch_ranks_multi): each
+    matrix is placed whole on one device by footprint, each device runs one
+    batch.  Returns (ranks, device per matrix)."""
+    keep = []
+    nm = len(mats)
+    m = np.array([int(x[3]) for x in mats], np.int64)
+    n = np.array([int(x[4]) for x in mats], np.int64)
+    devs = np.ascontiguousarray(devices, np.int32)
+    ranks = np.zeros(nm, np.int64)
+    where = np.zeros(nm, np.int32)
+    check(lib().rr_batch_ranks_multi(ptr(devs), devs.size, nm, ptr(m), ptr(n),
+                                     _pointer_arrays(keep, [x[0] for x in mats], np.int64),
+                                     _pointer_arrays(keep, [x[1] for x in mats], np.int32),
+                                     _pointer_arrays(keep, [x[2] for x in mats], np.uint32), int(theprime), int(num_v),
+                                     _pointer_arrays(keep, row_preconds, np.uint32),
+                                     _pointer_arrays(keep, col_preconds, np.uint32), _pointer_arrays(keep, vs, np.uint32),
+                                     int(workers), ptr(ranks), ptr(where)))
+    return ranks, where
+
+
+class Fleet(Server):
+    """Rank services on several GPUs (rr_fleet_*): each request is placed on
+    the device whose service has the most budget left, and follows
+    :class:`Server`'s path there."""
+
+    def __init__(self, num_v: int, theprime: int = DEFAULT_PRIME, devices=(0,), lanes: int = 4, workers: int = 4,
+                 max_active: int = 64, chunk_apps: int = 64, hbm_budget: int = 0):
+        from ._lib import ServerConfig
+
+        cfg = ServerConfig(int(num_v), int(theprime), int(lanes), int(workers), int(max_active), int(chunk_apps),
+                           int(hbm_budget))
+        devs = np.ascontiguousarray(devices, np.int32)
+        h = C.c_void_p()
+        check(lib().rr_fleet_create(ptr(devs), devs.size, C.byref(cfg), C.byref(h)))
+        self.handle = h
+        self.b = int(num_v)
+        _track(self, 0)
+
+    def submit(self, rowptr, col, val, m: int, n: int, row_precond, col_precond, v) -> int:
+        rowptr = np.ascontiguousarray(rowptr, np.int64)
+        col = np.ascontiguousarray(col, np.int32)
+        val = np.ascontiguousarray(val, np.uint32)
+        rp = np.ascontiguousarray(row_precond, np.uint32)
+        cp = np.ascontiguousarray(col_precond, np.uint32)
+        v = np.ascontiguousarray(v, np.uint32)
+        if rp.size != m or cp.size != n or v.shape != (self.b, n):
+            raise ValueError("preconditioner or block shapes do not match the matrix")
+        rid = C.c_uint64()
+        check(lib().rr_fleet_submit(self.handle, m, n, ptr(rowptr), ptr(col), ptr(val), ptr(rp), ptr(cp), ptr(v),
+                                    C.byref(rid)))
+        return rid.value
+
+    def result(self, rid: int, timeout: float = -1.0):
+        r, lat = C.c_int64(), C.c_double()
+        check(lib().rr_fleet_wait(self.handle, rid, float(timeout), C.byref(r), C.byref(lat)))
+        return r.value, lat.value
+
+    def device_of(self, rid: int) -> int:
+        d = C.c_int32()
+        check(lib().rr_fleet_device_of(self.handle, rid, C.byref(d)))
+        return d.value
+
+    def stats(self):
+        a, b = C.c_int64(), C.c_int64()
+        p50, p99, rps = C.c_double(), C.c_double(), C.c_double()
+        check(lib().rr_fleet_stats(self.handle, C.byref(a), C.byref(b), C.byref(p50), C.byref(p99), C.byref(rps)))
+        return {"submitted": a.value, "completed": b.value, "p50_ms": p50.value, "p99_ms": p99.value,
+                "ranks_per_s": rps.value}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().rr_fleet_destroy(self.handle)
+            self.handle = None
+
+
 def save_wdm_file_sym(path: str, n_rows: int, n_cols: int, theprime: int, row_precond, col_precond, v, curv, seq):
     """src/wdm_files.rs:126-210."""
     v = np.ascontiguousarray(v, np.uint32)

@@ -72,6 +72,17 @@ SIGNATURES = {
     "rr_server_stats": (C.c_int, [_vp, _pi64, _pi64, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                   C.POINTER(C.c_double)]),
     "rr_server_destroy": (C.c_int, [_vp]),
+    "rr_footprint": (C.c_int, [_i64, _i64, _i64, _i32, C.POINTER(C.c_uint64)]),
+    "rr_place_by_footprint": (C.c_int, [_i32, _vp, _i32, _vp, _vp, _vp]),
+    "rr_fleet_create": (C.c_int, [_vp, _i32, _vp, C.POINTER(_vp)]),
+    "rr_fleet_submit": (C.c_int, [_vp, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp, C.POINTER(C.c_uint64)]),
+    "rr_fleet_wait": (C.c_int, [_vp, C.c_uint64, C.c_double, _pi64, C.POINTER(C.c_double)]),
+    "rr_fleet_device_of": (C.c_int, [_vp, C.c_uint64, _pi32]),
+    "rr_fleet_stats": (C.c_int, [_vp, _pi64, _pi64, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                 C.POINTER(C.c_double)]),
+    "rr_fleet_destroy": (C.c_int, [_vp]),
+    "rr_batch_ranks_multi": (C.c_int, [_vp, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _u32, _i32, _vp, _vp, _vp, _i32,
+                                       _vp, _vp]),
 }
 
 

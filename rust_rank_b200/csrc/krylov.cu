@@ -994,158 +994,4 @@ int launch_scatter_block(rr_krylov* kr, const uint32_t* d_V, uint32_t* d_out) {
   return RR_OK;
 }
 
-// ---------------------------------------------------------------- matrix build
-// Host preprocessing: degree-ordered renumbering of rows and columns, the
-// transpose by counting sort (src/matrices.rs:734-778) and the chunk lists of
-// long rows; then one upload.
-namespace {
-
-struct HostCsr {
-  std::vector<uint32_t> ptr;
-  std::vector<uint2> cv;  // (column, value)
-  int64_t rows = 0, cols = 0;
-};
-
-// Indices by decreasing degree, ties in index order (a stable sort), by a
-// counting sort over the degrees.
-std::vector<int32_t> degree_order(const std::vector<int64_t>& deg) {
-  const int64_t n = (int64_t)deg.size();
-  int64_t maxd = 0;
-  for (int64_t d : deg) maxd = std::max(maxd, d);
-  std::vector<int64_t> start(maxd + 2, 0);  // bucket maxd - d holds degree d
-  for (int64_t d : deg) start[maxd - d + 1]++;
-  for (int64_t b = 0; b <= maxd; ++b) start[b + 1] += start[b];
-  std::vector<int32_t> order(n);
-  for (int64_t i = 0; i < n; ++i) order[start[maxd - deg[i]]++] = (int32_t)i;
-  return order;
-}
-
-// CSR of the transpose, stable by row (entries of a column in increasing row
-// order), on the host's cores: blocks of rows count their columns, each
-// (block, column) pair gets its own output range, and the blocks scatter in
-// parallel.
-void transpose_host(const HostCsr& a, HostCsr& t) {
-  t.rows = a.cols;
-  t.cols = a.rows;
-  t.ptr.assign(a.cols + 1, 0);
-  t.cv.resize(a.cv.size());
-  const int64_t hw = std::max(1u, std::thread::hardware_concurrency());
-  // at most 2^26 counters in all
-  const int64_t nblk =
-      std::max<int64_t>(1, std::min<int64_t>({hw, a.rows / 4096, ((int64_t)1 << 26) / std::max<int64_t>(a.cols, 1)}));
-  std::vector<uint32_t> cnt((size_t)nblk * a.cols, 0);
-  auto rlo = [&](int64_t b) { return a.rows * b / nblk; };
-  host_parallel_ranges(nblk, 1, [&](int64_t b0, int64_t b1) {
-    for (int64_t b = b0; b < b1; ++b) {
-      uint32_t* c = cnt.data() + (size_t)b * a.cols;
-      for (uint32_t k = a.ptr[rlo(b)]; k < a.ptr[rlo(b + 1)]; ++k) c[a.cv[k].x]++;
-    }
-  });
-  for (int64_t b = 0; b < nblk; ++b) {
-    const uint32_t* c = cnt.data() + (size_t)b * a.cols;
-    for (int64_t i = 0; i < a.cols; ++i) t.ptr[i + 1] += c[i];
-  }
-  for (int64_t i = 0; i < a.cols; ++i) t.ptr[i + 1] += t.ptr[i];
-  // counts -> first output position of each (block, column)
-  host_parallel_ranges(a.cols, (int64_t)1 << 14, [&](int64_t c0, int64_t c1) {
-    for (int64_t c = c0; c < c1; ++c) {
-      uint32_t run = t.ptr[c];
-      for (int64_t b = 0; b < nblk; ++b) {
-        uint32_t& x = cnt[(size_t)b * a.cols + c];
-        const uint32_t k = x;
-        x = run;
-        run += k;
-      }
-    }
-  });
-  host_parallel_ranges(nblk, 1, [&](int64_t b0, int64_t b1) {
-    for (int64_t b = b0; b < b1; ++b) {
-      uint32_t* next = cnt.data() + (size_t)b * a.cols;
-      for (int64_t r = rlo(b); r < rlo(b + 1); ++r)
-        for (uint32_t k = a.ptr[r]; k < a.ptr[r + 1]; ++k) t.cv[next[a.cv[k].x]++] = make_uint2((uint32_t)r, a.cv[k].y);
-    }
-  });
-}
-
-int upload_csr(const HostCsr& h, DevCsr& d, cudaStream_t s) {
-  d.rows = h.rows;
-  d.cols = h.cols;
-  d.nnz = (int64_t)h.cv.size();
-  RR_TRY(d.rowptr.alloc_async(h.ptr.size(), s));
-  RR_TRY(d.cv.alloc_async(std::max<size_t>(h.cv.size(), 1), s));
-  RR_CUDA(cudaMemcpyAsync(d.rowptr.ptr, h.ptr.data(), h.ptr.size() * 4, cudaMemcpyHostToDevice, s));
-  if (!h.cv.empty())
-    RR_CUDA(cudaMemcpyAsync(d.cv.ptr, h.cv.data(), h.cv.size() * sizeof(uint2), cudaMemcpyHostToDevice, s));
-  // long rows form a prefix (rows are sorted by decreasing degree)
-  int64_t heavy = 0;
-  while (heavy < h.rows && (int64_t)(h.ptr[heavy + 1] - h.ptr[heavy]) > kHeavyDegree) ++heavy;
-  d.heavy_rows = heavy;
-  struct Chunk { uint32_t row, beg, end, key; };
-  std::vector<Chunk> chunks;
-  for (int64_t r = 0; r < heavy; ++r)
-    for (uint32_t k = h.ptr[r]; k < h.ptr[r + 1]; k += (uint32_t)kChunkNnz) {
-      const uint32_t e = std::min<uint32_t>(h.ptr[r + 1], k + (uint32_t)kChunkNnz);
-      chunks.push_back({(uint32_t)r, k, e, h.cv[k].x});
-    }
-  // chunks that gather the same region of the input block run together
-  std::stable_sort(chunks.begin(), chunks.end(), [](const Chunk& a, const Chunk& b) { return a.key < b.key; });
-  d.nchunks = (int64_t)chunks.size();
-  if (d.nchunks) {
-    std::vector<uint32_t> cr(d.nchunks), cb(d.nchunks), ce(d.nchunks);
-    for (int64_t i = 0; i < d.nchunks; ++i) { cr[i] = chunks[i].row; cb[i] = chunks[i].beg; ce[i] = chunks[i].end; }
-    RR_TRY(d.chunk_row.alloc_async(d.nchunks, s));
-    RR_TRY(d.chunk_begin.alloc_async(d.nchunks, s));
-    RR_TRY(d.chunk_end.alloc_async(d.nchunks, s));
-    RR_CUDA(cudaMemcpyAsync(d.chunk_row.ptr, cr.data(), d.nchunks * 4, cudaMemcpyHostToDevice, s));
-    RR_CUDA(cudaMemcpyAsync(d.chunk_begin.ptr, cb.data(), d.nchunks * 4, cudaMemcpyHostToDevice, s));
-    RR_CUDA(cudaMemcpyAsync(d.chunk_end.ptr, ce.data(), d.nchunks * 4, cudaMemcpyHostToDevice, s));
-    RR_CUDA(cudaStreamSynchronize(s));  // host vectors die at scope end
-  }
-  RR_CUDA(cudaStreamSynchronize(s));
-  return RR_OK;
-}
-
-}  // namespace
-
-int matrix_build(rr_ctx* ctx, int64_t m, int64_t n, const int64_t* rowptr, const int32_t* col, const uint32_t* val,
-                 uint32_t p, rr_matrix* mat) {
-  const int64_t nnz = rowptr[m];
-  std::vector<int64_t> rdeg(m), cdeg(n, 0);
-  for (int64_t r = 0; r < m; ++r) rdeg[r] = rowptr[r + 1] - rowptr[r];
-  for (int64_t k = 0; k < nnz; ++k) cdeg[col[k]]++;
-  mat->max_row_nnz = m ? *std::max_element(rdeg.begin(), rdeg.end()) : 0;
-  mat->max_col_nnz = n ? *std::max_element(cdeg.begin(), cdeg.end()) : 0;
-  mat->rowperm = degree_order(rdeg);
-  mat->colperm = degree_order(cdeg);
-  std::vector<int32_t> inv_col(n);
-  for (int64_t c = 0; c < n; ++c) inv_col[mat->colperm[c]] = (int32_t)c;
-
-  HostCsr A;
-  A.rows = m;
-  A.cols = n;
-  A.ptr.resize(m + 1);
-  A.cv.resize(nnz);
-  A.ptr[0] = 0;
-  for (int64_t rp = 0; rp < m; ++rp) A.ptr[rp + 1] = A.ptr[rp] + (uint32_t)rdeg[mat->rowperm[rp]];
-  // rows in their new order, columns renumbered and sorted; rows are independent
-  host_parallel_ranges(m, (int64_t)1 << 12, [&](int64_t lo, int64_t hi) {
-    for (int64_t rp = lo; rp < hi; ++rp) {
-      const int64_t r = mat->rowperm[rp];
-      uint32_t o = A.ptr[rp];
-      for (int64_t k = rowptr[r]; k < rowptr[r + 1]; ++k) A.cv[o++] = make_uint2((uint32_t)inv_col[col[k]], val[k]);
-      std::sort(A.cv.begin() + A.ptr[rp], A.cv.begin() + o, [](const uint2& a, const uint2& b) { return a.x < b.x; });
-    }
-  });
-  HostCsr At;
-  transpose_host(A, At);
-  cudaStream_t s = ctx->stream;
-  RR_TRY(upload_csr(A, mat->A, s));
-  RR_TRY(upload_csr(At, mat->At, s));
-  RR_TRY(mat->d_colperm.alloc_async(std::max<int64_t>(n, 1), s));
-  RR_CUDA(cudaMemcpyAsync(mat->d_colperm.ptr, mat->colperm.data(), n * 4, cudaMemcpyHostToDevice, s));
-  RR_CUDA(cudaStreamSynchronize(s));
-  (void)p;
-  return RR_OK;
-}
-
 }  // namespace rr

@@ -154,9 +154,8 @@ struct rr_matrix_s {
   int64_t max_row_nnz = 0, max_col_nnz = 0;
   rr::DevCsr A;   // rows of A in degree order, columns renumbered in degree order
   rr::DevCsr At;  // its transpose
-  std::vector<int32_t> rowperm;  // rowperm[r'] = original row
-  std::vector<int32_t> colperm;  // colperm[c'] = original column
-  rr::DevBuf<int32_t> d_colperm;
+  rr::DevBuf<int32_t> d_rowperm;  // d_rowperm[r'] = original row
+  rr::DevBuf<int32_t> d_colperm;  // d_colperm[c'] = original column
 };
 
 struct rr_krylov_s {
@@ -199,8 +198,29 @@ int krylov_reserve(rr_krylov* kr, int64_t terms);
 int krylov_launch_application(rr_krylov* kr, cudaEvent_t* ev);
 int krylov_launch_get_curv(rr_krylov* kr, uint32_t* d_out);
 int krylov_occupancy(rr_krylov* kr);
-int matrix_build(rr_ctx* ctx, int64_t m, int64_t n, const int64_t* rowptr, const int32_t* col,
-                 const uint32_t* val, uint32_t p, rr_matrix* mat);
+// Sequence length rule of src/main.rs:497-504; padded block width; device
+// bytes a matrix and its Krylov state hold while resident (server.cpp).
+int64_t max_nlen_for(int64_t m, int64_t n, int b);
+int padded(int b);
+size_t footprint_of(int64_t m, int64_t n, int64_t nnz, int b, int64_t max_nlen);
+struct ServerSnapshot {
+  std::vector<double> latencies_ms;
+  int64_t submitted = 0, completed = 0;
+  double t_first = 0, t_last = 0;  // seconds on the steady clock
+  uint64_t hbm_budget = 0;
+};
+void server_snapshot(rr_server* s, ServerSnapshot* out);
+// Greedy placement by footprint: items in decreasing size order, each on the
+// device with the most room left (ties: lowest index).  With allow_over, an
+// item that fits nowhere goes to the device with the most room anyway;
+// otherwise that is RR_ENOMEM.  device_of[i] receives item i's device index.
+int place_by_footprint(int nitems, const uint64_t* footprint, int ndev, const uint64_t* dev_free, bool allow_over,
+                       int32_t* device_of, uint64_t* dev_load);
+
+// The degree-ordered CSR of A and of its transpose, built on the device
+// (build.cu); validates the input (RR_EINVAL with the first bad index).
+int matrix_build_device(rr_ctx* ctx, int64_t m, int64_t n, const int64_t* rowptr, const int32_t* col,
+                        const uint32_t* val, uint32_t p, rr_matrix* mat);
 // PM-basis on the device; M (host) [2b][2b][d+1], delta (host) [2b].
 int pm_basis_device(rr_ctx* ctx, const uint32_t* seq, int64_t seq_stride, int b, int64_t nlen, int64_t d,
                     uint32_t p, uint32_t* M, int64_t* delta);

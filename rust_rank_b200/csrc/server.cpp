@@ -77,6 +77,10 @@ struct Request {
   Clock::time_point t_submit, t_ready, t_done;
 };
 
+}  // namespace
+
+namespace rr {
+
 // Sequence length rule of src/main.rs:497-504.
 int64_t max_nlen_for(int64_t m, int64_t n, int b) {
   int64_t L = (int64_t)std::floor(2.0f * (float)std::min(m, n) / (float)b + 4.0f);
@@ -102,6 +106,12 @@ size_t footprint_of(int64_t m, int64_t n, int64_t nnz, int b, int64_t max_nlen) 
   return (size_t)((double)(csr + blocks + heavy + seq) * 1.1) + (1u << 20);
 }
 
+}  // namespace rr
+
+namespace {
+using rr::footprint_of;
+using rr::max_nlen_for;
+using rr::padded;
 }  // namespace
 
 struct rr_server_s {
@@ -384,6 +394,16 @@ struct rr_server_s {
 };
 
 using namespace rr;
+
+void rr::server_snapshot(rr_server* s, ServerSnapshot* out) {
+  std::lock_guard<std::mutex> lk(s->mu);
+  out->latencies_ms = s->latencies_ms;
+  out->submitted = s->submitted;
+  out->completed = s->completed;
+  out->t_first = std::chrono::duration<double>(s->t_first.time_since_epoch()).count();
+  out->t_last = std::chrono::duration<double>(s->t_last.time_since_epoch()).count();
+  out->hbm_budget = s->cfg.hbm_budget;
+}
 
 extern "C" {
 
