@@ -215,8 +215,11 @@ int rr_batch_create(rr_ctx* ctx, int32_t nmat, const int64_t* m, const int64_t* 
                     const uint32_t* const* row_precond, const uint32_t* const* col_precond,
                     const uint32_t* const* V, rr_batch** out);
 int rr_batch_destroy(rr_batch* batch);
-/* All Krylov sequences: S_0 for every matrix, then one launch per pass of B
- * over the matrices whose sequences are still running.  Once per batch. */
+/* All Krylov sequences: S_0 for every matrix, then one persistent
+ * cooperative launch per phase (the applications between two sequence ends)
+ * that runs both passes of every application with grid-wide barriers between
+ * them, all captured into one CUDA graph.  RR_ETIMEOUT when a barrier wait
+ * gave up (2 s).  Once per batch. */
 int rr_batch_krylov(rr_batch* batch);
 /* Sequence of matrix i: *len = its length; seq [b(b+1)/2][seq_stride >= len]
  * (src/main.rs:164-175 order), or NULL to query the length only. */
@@ -227,14 +230,23 @@ int rr_batch_sequence(rr_batch* batch, int32_t i, uint32_t* seq, int64_t seq_str
 int rr_batch_ranks(rr_batch* batch, int32_t workers, int64_t* ranks);
 /* Launch shapes the batch's autotuner picked: the Krylov loop has one phase
  * per distinct set of running matrices (phase k covers applications
- * apps_from[k] .. apps_from[k+1]-1); ctas[k] is the grid of its pass launches,
- * chosen at create time by timing 1..4 CTAs per SM.  Call with NULL arrays to
- * get the phase count; *nphases gives the room of the arrays. */
+ * apps_from[k] .. apps_from[k+1]-1); ctas[k] is the grid of its persistent
+ * launch, chosen at create time by timing 1..(co-resident maximum) CTAs per
+ * SM.  Call with NULL arrays to get the phase count; *nphases gives the room
+ * of the arrays. */
 int rr_batch_tuning(const rr_batch* batch, int32_t* nphases, int32_t* ctas, int64_t* apps_from);
 /* Stacked sizes: rows and columns with padding, nonzeros, applications of
  * B of the longest sequence. */
 int rr_batch_info(const rr_batch* batch, int64_t* total_rows, int64_t* total_cols, int64_t* total_nnz,
                   int64_t* max_apps);
+/* Check of the device-side grid barrier the batch's persistent Krylov launch
+ * uses (no counterpart in the reference): a cooperative launch of `ctas` CTAs
+ * passes `rounds` barriers that each wait for `expected` arrivals, giving up
+ * after limit_s seconds (0 < limit_s <= 10).  *timed_out = 1 when a wait gave
+ * up (expected > ctas makes every wait run out), 0 otherwise; the context
+ * stays usable either way.  ctas must fit on the device at once. */
+int rr_device_barrier_check(rr_ctx* ctx, int32_t ctas, int32_t expected, int32_t rounds, double limit_s,
+                            int32_t* timed_out);
 
 /* ---------------------------------------------------------------- serving */
 /* A rank service: requests (one matrix each, with its preconditioners and V)

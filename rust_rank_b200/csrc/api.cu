@@ -460,6 +460,26 @@ int rr_krylov_fill_status(rr_krylov* kr, char* buf, int64_t cap) {
   return RR_OK;
 }
 
+int rr_device_barrier_check(rr_ctx* ctx, int32_t ctas, int32_t expected, int32_t rounds, double limit_s,
+                            int32_t* timed_out) {
+  if (!ctx || !timed_out || ctas < 1 || expected < 1 || rounds < 1 || !(limit_s > 0) || limit_s > 10)
+    return fail(RR_EINVAL, "bad argument");
+  RR_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  DevBuf<unsigned int> bar;
+  DevBuf<int> err;
+  RR_TRY(bar.alloc_async(2, s));
+  RR_TRY(err.alloc_async(1, s));
+  RR_CUDA(cudaMemsetAsync(bar.ptr, 0, 2 * sizeof(unsigned int), s));
+  RR_CUDA(cudaMemsetAsync(err.ptr, 0, sizeof(int), s));
+  RR_TRY(launch_barrier_check(s, ctas, bar.ptr, err.ptr, (uint64_t)(limit_s * 1e9), (unsigned)expected, rounds));
+  int e = 0;
+  RR_CUDA(cudaMemcpyAsync(&e, err.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
+  RR_CUDA(cudaStreamSynchronize(s));
+  *timed_out = e;
+  return RR_OK;
+}
+
 int rr_krylov_length(const rr_krylov* kr, int64_t* len) {
   if (!kr || !len) return fail(RR_EINVAL, "NULL argument");
   *len = kr->len;

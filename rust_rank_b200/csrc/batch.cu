@@ -7,7 +7,12 @@
 // terms are accumulated in segments (krylov.cu, batched mode).  Matrices are
 // stacked by increasing sequence length, so the matrices still running at
 // application t form a suffix of the stack and the passes start at that
-// suffix.  Each application of B is then two launches for the whole batch.
+// suffix.  A phase (the applications between two sequence ends, over one set
+// of running matrices) is ONE persistent cooperative launch: the CTAs walk
+// the stacked rows of A, meet at a grid-wide barrier, walk the rows of A^T,
+// meet again, for every application of the phase.  The whole Krylov loop
+// (the initial pass, one launch per phase and the term finalisations) is
+// captured once into a CUDA graph and launched as one graph.
 //
 // The generators: matrices with equal sequence length finish their Krylov
 // loops together and are solved in lockstep by one batched PM-basis (one
@@ -58,6 +63,8 @@ struct rr_batch_s {
   rr::DevBuf<unsigned int> counter;
   rr::DevBuf<uint32_t> S;
   rr::DevBuf<int64_t> d_s_off;
+  rr::DevBuf<unsigned int> bar;  // grid barrier of the persistent launches: arrivals, generation
+  rr::DevBuf<int> error;         // set when a barrier wait gives up
   int64_t nnz = 0;
   int cur = 0;
   bool done = false;
@@ -153,47 +160,69 @@ void phase_runs(const rr_batch* bt, int ph, int grid, const std::vector<int64_t>
   equal_runs(wt, bt->col_off[f] / rpb, bt->col_off[bt->nmat] / rpb, nw, rt);
 }
 
-// One application of B over the matrices of phase ph (the Krylov loop's two
-// launches), with the given grid and run tables.
-int launch_phase_app(rr_batch* bt, int ph, int grid, const int32_t* d_ra, const int32_t* d_rt, int64_t t) {
+// A grid-wide barrier wait gives up after this long (the whole phase then
+// stops and rr_batch_krylov / rr_batch_ranks return RR_ETIMEOUT).
+constexpr uint64_t kBarrierLimitNs = 2000000000ull;
+
+// Parameters of the persistent launch of phase ph for applications
+// [t_begin, t_end) with the given grid and warp-run tables.
+PersistParams phase_params(rr_batch* bt, int ph, const int32_t* d_ra, const int32_t* d_rt, int64_t t_begin,
+                           int64_t t_end, int cur0) {
   const int rpb = rows_per_batch(bt->B), nmat = bt->nmat, first = bt->phase_first[ph];
+  PersistParams Q;
+  std::memset(&Q, 0, sizeof(Q));
   PassParams P = batch_params(bt);
   P.seg_begin = first;
   P.seg_end = nmat;
   P.replicas = std::max(1, std::min(kGramReplicas, 64 / (nmat - first)));
+  // rows of A: z = A x, U = D_r z, odd term
   P.rowptr = bt->A.rowptr.ptr;
   P.cv = bt->A.cv.ptr;
   P.rows = bt->row_off[nmat];
-  P.X = reinterpret_cast<const uint4*>(bt->X[bt->cur].ptr);
-  P.Y = reinterpret_cast<uint4*>(bt->U.ptr);
   P.scale = bt->dr_m.ptr;
   P.gram_mul = bt->M.r1;
   P.batch_seg = bt->seg_rows.ptr;
   P.runs = d_ra;
   P.batch_begin = bt->row_off[first] / rpb;
-  P.term = 2 * t + 1;
-  RR_TRY(launch_pass_raw(bt->stream, bt->B, bt->fold4, grid, P, kModeOdd));
+  Q.odd = P;
+  // rows of A^T: w' = D_c A^T U, x' = D_c w', even term
   P.rowptr = bt->At.rowptr.ptr;
   P.cv = bt->At.cv.ptr;
   P.rows = bt->col_off[nmat];
-  P.X = reinterpret_cast<const uint4*>(bt->U.ptr);
-  P.Y = reinterpret_cast<uint4*>(bt->X[bt->cur ^ 1].ptr);
   P.scale = bt->dc_m.ptr;
   P.scale2 = bt->dc_r.ptr;
   P.gram_mul = 1;
   P.batch_seg = bt->seg_cols.ptr;
   P.runs = d_rt;
   P.batch_begin = bt->col_off[first] / rpb;
-  P.term = 2 * t + 2;
-  return launch_pass_raw(bt->stream, bt->B, bt->fold4, grid, P, kModeEven);
+  Q.even = P;
+  Q.X[0] = reinterpret_cast<uint4*>(bt->X[0].ptr);
+  Q.X[1] = reinterpret_cast<uint4*>(bt->X[1].ptr);
+  Q.U = reinterpret_cast<uint4*>(bt->U.ptr);
+  Q.cur0 = cur0;
+  Q.t_begin = t_begin;
+  Q.t_end = t_end;
+  Q.bar = bt->bar.ptr;
+  Q.error = bt->error.ptr;
+  Q.limit_ns = kBarrierLimitNs;
+  return Q;
 }
 
-// Autotuner: for every phase, time a few applications of B with 1..`max_cps`
-// CTAs per SM and keep the fastest.  Few or small running matrices leave
-// each warp only a few row batches on the full grid, and the per-warp fixed
-// costs (Gram set-up, flush, atomics) then dominate; a smaller grid amortises
-// them.  The timed applications write terms 1 and 2 of the running matrices
-// and scratch blocks only; the Krylov loop recomputes all of them.
+int launch_phase(rr_batch* bt, int ph, int grid, const int32_t* d_ra, const int32_t* d_rt, int64_t t_begin,
+                 int64_t t_end, int cur0) {
+  PersistParams Q = phase_params(bt, ph, d_ra, d_rt, t_begin, t_end, cur0);
+  RR_CUDA(cudaMemsetAsync(bt->bar.ptr, 0, 2 * sizeof(unsigned int), bt->stream));
+  return launch_persistent_raw(bt->stream, bt->B, bt->fold4, grid, Q);
+}
+
+// Autotuner: for every phase, time a persistent launch of three
+// applications of B with 1..`max_cps` co-resident CTAs per SM and keep the
+// fastest.  Few or small running matrices leave each warp only a few row
+// batches on the full grid, and the per-warp fixed costs (Gram set-up, flush,
+// atomics) and the barriers then dominate; a smaller grid amortises them.
+// The timed applications write terms 1..6 of the running matrices and
+// scratch blocks only; the slots are cleared and the Krylov loop recomputes
+// all of them.
 int tune_phases(rr_batch* bt, int max_cps, const std::vector<int64_t>& wa, const std::vector<int64_t>& wt) {
   const int nph = (int)bt->phase_first.size(), sms = bt->ctx->num_sms;
   const int max_grid = std::max(1, max_cps) * sms;
@@ -220,9 +249,9 @@ int tune_phases(rr_batch* bt, int max_cps, const std::vector<int64_t>& wa, const
         status = fail(RR_ECUDA, "tuning upload failed");
         break;
       }
-      status = launch_phase_app(bt, ph, grid, dra.ptr, drt.ptr, 0);  // warm-up
+      status = launch_phase(bt, ph, grid, dra.ptr, drt.ptr, 0, 1, 0);  // warm-up
       if (status == RR_OK) cudaEventRecord(e0, bt->stream);
-      for (int rep = 0; rep < 3 && status == RR_OK; ++rep) status = launch_phase_app(bt, ph, grid, dra.ptr, drt.ptr, 0);
+      if (status == RR_OK) status = launch_phase(bt, ph, grid, dra.ptr, drt.ptr, 0, 3, 0);
       if (status != RR_OK) break;
       cudaEventRecord(e1, bt->stream);
       if (cudaEventSynchronize(e1) != cudaSuccess) {
@@ -262,11 +291,13 @@ struct Progress {
   bool failed = false;
 };
 
-// The whole Krylov loop on the batch's stream.  With ev, the event of stack
-// position s is recorded after its last application and s is published.
-int krylov_run(rr_batch* bt, cudaEvent_t* ev, Progress* prog) {
+// The whole Krylov loop on the batch's stream: S_0 and x = D_c V for every
+// matrix, then one persistent launch per phase, each followed by the
+// finalisation of the terms of the matrices whose sequences end there (and,
+// with ev, the record of their events; stack position s is then published).
+// The launches are captured into one CUDA graph and launched once.
+int krylov_queue(rr_batch* bt, cudaEvent_t* ev) {
   cudaStream_t st = bt->stream;
-  const int rpb = rows_per_batch(bt->B);
   const int nmat = bt->nmat;
   {  // x = D_c V and S_0 for every matrix
     PassParams P = batch_params(bt);
@@ -281,65 +312,67 @@ int krylov_run(rr_batch* bt, cudaEvent_t* ev, Progress* prog) {
     P.term = 0;
     RR_TRY(launch_pass_raw(st, bt->B, bt->fold4, bt->grid, P, kModeInit));
   }
-  bt->cur = 0;
+  RR_CUDA(cudaMemsetAsync(bt->error.ptr, 0, sizeof(int), st));
   const int64_t max_apps = bt->apps[nmat - 1];
-  int first = 0;
-  for (int64_t t = 0; t < max_apps; ++t) {
+  int first = 0, cur = 0;
+  int64_t t = 0;
+  while (t < max_apps) {
     while (first < nmat && bt->apps[first] <= t) ++first;
     const int ph = bt->phase_of[first];
+    const int64_t t_end = bt->apps[first];  // the next sequence end
     const size_t run_off = (size_t)bt->run_off[ph];
-    const int grid = bt->phase_grid[ph];
-    uint32_t* x = bt->X[bt->cur].ptr;
-    uint32_t* xn = bt->X[bt->cur ^ 1].ptr;
-    PassParams P = batch_params(bt);
-    P.seg_begin = first;
-    P.seg_end = nmat;
-    // few running matrices: spread their accumulators over replicas
-    P.replicas = std::max(1, std::min(kGramReplicas, 64 / (nmat - first)));
-    // rows of A: z = A x, U = D_r z, odd term
-    P.rowptr = bt->A.rowptr.ptr;
-    P.cv = bt->A.cv.ptr;
-    P.rows = bt->row_off[nmat];
-    P.X = reinterpret_cast<const uint4*>(x);
-    P.Y = reinterpret_cast<uint4*>(bt->U.ptr);
-    P.scale = bt->dr_m.ptr;
-    P.gram_mul = bt->M.r1;
-    P.batch_seg = bt->seg_rows.ptr;
-    P.runs = bt->runs_rows.ptr + run_off;
-    P.batch_begin = bt->row_off[first] / rpb;
-    P.term = 2 * t + 1;
-    RR_TRY(launch_pass_raw(st, bt->B, bt->fold4, grid, P, kModeOdd));
-    // rows of A^T: w' = D_c A^T U, x' = D_c w', even term
-    P.rowptr = bt->At.rowptr.ptr;
-    P.cv = bt->At.cv.ptr;
-    P.rows = bt->col_off[nmat];
-    P.X = reinterpret_cast<const uint4*>(bt->U.ptr);
-    P.Y = reinterpret_cast<uint4*>(xn);
-    P.scale = bt->dc_m.ptr;
-    P.scale2 = bt->dc_r.ptr;
-    P.gram_mul = 1;
-    P.batch_seg = bt->seg_cols.ptr;
-    P.runs = bt->runs_cols.ptr + run_off;
-    P.batch_begin = bt->col_off[first] / rpb;
-    P.term = 2 * t + 2;
-    RR_TRY(launch_pass_raw(st, bt->B, bt->fold4, grid, P, kModeEven));
-    bt->cur ^= 1;
-    // matrices whose sequences end here: finish their terms, then publish
+    RR_TRY(launch_phase(bt, ph, bt->phase_grid[ph], bt->runs_rows.ptr + run_off, bt->runs_cols.ptr + run_off, t, t_end,
+                        cur));
+    cur ^= (int)((t_end - t) & 1);
+    t = t_end;
+    // matrices whose sequences end here: finish their terms
     int done_to = first;
-    while (done_to < nmat && bt->apps[done_to] == t + 1) ++done_to;
-    if (done_to > first) {
-      RR_TRY(launch_batch_finalize(st, bt->gram_all.ptr, bt->d_seg_G_off.ptr, bt->S.ptr, bt->d_s_off.ptr,
-                                   bt->d_seg_terms.ptr, first, done_to, 2 * (t + 1) + 1, bt->b, bt->B, bt->M));
-      if (ev) {
-        for (int s = first; s < done_to; ++s) RR_CUDA(cudaEventRecord(ev[s], st));
-        {
-          std::lock_guard<std::mutex> lk(prog->mu);
-          prog->published = done_to;
-        }
-        prog->cv.notify_all();
-      }
-    }
+    while (done_to < nmat && bt->apps[done_to] == t) ++done_to;
+    RR_TRY(launch_batch_finalize(st, bt->gram_all.ptr, bt->d_seg_G_off.ptr, bt->S.ptr, bt->d_s_off.ptr,
+                                 bt->d_seg_terms.ptr, first, done_to, 2 * t + 1, bt->b, bt->B, bt->M));
+    if (ev)
+      for (int s = first; s < done_to; ++s) RR_CUDA(cudaEventRecordWithFlags(ev[s], st, cudaEventRecordExternal));
   }
+  bt->cur = cur;
+  return RR_OK;
+}
+
+int krylov_run(rr_batch* bt, cudaEvent_t* ev, Progress* prog) {
+  cudaStream_t st = bt->stream;
+  cudaGraph_t g = nullptr;
+  RR_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  const int rc = krylov_queue(bt, ev);
+  const cudaError_t ec = cudaStreamEndCapture(st, &g);
+  if (rc != RR_OK) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  RR_CUDA(ec);
+  cudaGraphExec_t ge = nullptr;
+  const cudaError_t ei = cudaGraphInstantiate(&ge, g, 0);
+  cudaGraphDestroy(g);
+  RR_CUDA(ei);
+  const cudaError_t el = cudaGraphLaunch(ge, st);
+  cudaGraphExecDestroy(ge);  // released once the launch completes
+  RR_CUDA(el);
+  if (ev) {  // everything is queued: the events mark each sequence's completion
+    {
+      std::lock_guard<std::mutex> lk(prog->mu);
+      prog->published = bt->nmat;
+    }
+    prog->cv.notify_all();
+  }
+  return RR_OK;
+}
+
+// RR_ETIMEOUT when a grid barrier of the persistent launches gave up
+// (synchronises the batch's stream).
+int krylov_status(rr_batch* bt) {
+  int err = 0;
+  RR_CUDA(cudaMemcpyAsync(&err, bt->error.ptr, sizeof(int), cudaMemcpyDeviceToHost, bt->stream));
+  RR_CUDA(cudaStreamSynchronize(bt->stream));
+  if (err) return fail(RR_ETIMEOUT, "a grid barrier of the persistent Krylov launch gave up after %.1f s",
+                       (double)kBarrierLimitNs * 1e-9);
   return RR_OK;
 }
 
@@ -526,8 +559,13 @@ int rr_batch_create(rr_ctx* ctx, int32_t nmat, const int64_t* m, const int64_t* 
     RR_TRY(up(bt->d_seg_terms, terms));
     RR_TRY(bt->gram_all.alloc((size_t)std::max<int64_t>(goff[nmat], 1)));
   }
-  int blocks = 1;
+  RR_TRY(bt->bar.alloc(2));
+  RR_TRY(bt->error.alloc(1));
+  RR_CUDA(cudaMemsetAsync(bt->bar.ptr, 0, bt->bar.bytes(), st));
+  RR_CUDA(cudaMemsetAsync(bt->error.ptr, 0, bt->error.bytes(), st));
+  int blocks = 1, pblocks = 1;
   RR_TRY(pass_blocks_per_sm(bt->B, bt->fold4, &blocks));
+  RR_TRY(persistent_blocks_per_sm(bt->B, bt->fold4, &pblocks));
   bt->grid = std::max(1, blocks) * ctx->num_sms;
   // phases: one per distinct set of running matrices
   bt->phase_of.assign(nmat, -1);
@@ -541,7 +579,8 @@ int rr_batch_create(rr_ctx* ctx, int32_t nmat, const int64_t* m, const int64_t* 
   RR_CUDA(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
   RR_CUDA(cudaStreamCreateWithPriority(&bt->stream, cudaStreamNonBlocking, prio_hi));
   RR_CUDA(cudaStreamSynchronize(st));
-  RR_TRY(tune_phases(bt.get(), blocks, wa, wt));
+  RR_TRY(tune_phases(bt.get(), std::max(1, pblocks), wa, wt));
+  RR_TRY(krylov_status(bt.get()));
   RR_CUDA(cudaMemsetAsync(bt->gram_all.ptr, 0, bt->gram_all.bytes(), bt->stream));
   RR_CUDA(cudaStreamSynchronize(bt->stream));
   RR_CUDA(cudaStreamSynchronize(st));
@@ -579,7 +618,7 @@ int rr_batch_krylov(rr_batch* bt) {
   if (bt->done) return fail(RR_ESTATE, "the batch's sequences were already computed");
   RR_CUDA(cudaSetDevice(bt->ctx->device));
   RR_TRY(krylov_run(bt, nullptr, nullptr));
-  RR_CUDA(cudaStreamSynchronize(bt->stream));
+  RR_TRY(krylov_status(bt));
   bt->done = true;
   return RR_OK;
 }
@@ -717,6 +756,10 @@ int rr_batch_ranks(rr_batch* bt, int32_t workers, int64_t* ranks) {
   }
   for (auto& th : pool) th.join();
   if (overlap) {
+    if (krc == RR_OK) {
+      krc = krylov_status(bt);
+      if (krc != RR_OK) kerr = rr_last_error();
+    }
     cudaStreamSynchronize(bt->stream);
     for (int s = 0; s < nmat; ++s) cudaEventDestroy(ev[s]);
     if (krc == RR_OK) bt->done = true;

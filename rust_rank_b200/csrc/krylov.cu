@@ -92,7 +92,16 @@ __device__ __forceinline__ void mac_step(const uint2 (&e)[4], const uint4 (&g)[4
 // next step loaded while the current step's gathers are in flight; the last,
 // partial step clamps its index into the row and multiplies by zero instead
 // of branching (the clamped gather re-reads a row already in cache).
-template <int B, int FE>
+// Gathers of the block: through the read-only path, or (COH, inside the
+// persistent batched kernel, where the block is rewritten between grid
+// barriers) from L2 with ordinary coherent loads.
+template <bool COH>
+__device__ __forceinline__ uint4 ld_block(const uint4* p) {
+  if (COH) return __ldcg(p);
+  return __ldg(p);
+}
+
+template <int B, int FE, bool COH = false>
 __device__ __forceinline__ void gather_sum(const uint2* __restrict__ cv, uint32_t beg, uint32_t end, uint32_t stride,
                                            const uint4* __restrict__ X, int sub, const ModP& M,
                                            uint64_t (&acc)[Shape<B>::LPT]) {
@@ -110,7 +119,7 @@ __device__ __forceinline__ void gather_sum(const uint2* __restrict__ cv, uint32_
 #pragma unroll
       for (int u = 0; u < 4; ++u)
 #pragma unroll
-        for (int v = 0; v < NV; ++v) g[u][v] = __ldg(Xs + (size_t)e[u].x * RW + v);
+        for (int v = 0; v < NV; ++v) g[u][v] = ld_block<COH>(Xs + (size_t)e[u].x * RW + v);
       k += step;
       const bool more = k + 3 * stride < end;
       uint2 en[4];
@@ -136,7 +145,7 @@ __device__ __forceinline__ void gather_sum(const uint2* __restrict__ cv, uint32_
 #pragma unroll
     for (int u = 0; u < 4; ++u)
 #pragma unroll
-      for (int v = 0; v < NV; ++v) g[u][v] = __ldg(Xs + (size_t)e[u].x * RW + v);
+      for (int v = 0; v < NV; ++v) g[u][v] = ld_block<COH>(Xs + (size_t)e[u].x * RW + v);
     mac_step<B, FE>(e, g, M, acc);
   }
 }
@@ -378,21 +387,17 @@ __device__ __forceinline__ unsigned long long* seg_target(const PassParams& P, u
   return acc + (size_t)sg * NP;
 }
 
-template <int B, int MODE, int FE>
-// Four CTAs (32 warps) per SM: the walk is latency bound, so occupancy is
-// worth a few spilled registers (measured on the 2M x 1.5M Zipf matrix).  At
-// B = 32 the Gram accumulators alone take 48 registers, and two CTAs per SM
-// with 128 registers run the same matrix 1.2x faster than four with spills.
-__global__ void __launch_bounds__(kThreads, (B >= 32 ? 2 : 4)) pass_kernel(PassParams P) {
+// One pass over the rows of A (MODE odd), of A^T (even) or the initial
+// scaling (init), by the whole CTA: gram_smem is the per-warp Gram staging,
+// red[NP] the CTA's Gram reduction, is_last a shared flag.
+template <int B, int MODE, int FE, bool COH>
+__device__ __forceinline__ void pass_body(const PassParams& P, uint32_t* gram_smem, unsigned long long* red,
+                                          bool& is_last) {
   using S = Shape<B>;
   constexpr int LPT = S::LPT, NV = S::NV, TPR = S::TPR, RPW = S::RPW;
   constexpr int NP = B * (B + 1) / 2;  // pairs in padded space
   constexpr bool kMma = B >= 8;
   using Gram = typename std::conditional<kMma, GramMma<B, FE>, GramCore<B, FE>>::type;
-
-  extern __shared__ __align__(16) uint32_t gram_smem[];
-  __shared__ unsigned long long red[NP];
-  __shared__ bool is_last;
 
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
@@ -457,7 +462,7 @@ __global__ void __launch_bounds__(kThreads, (B >= 32 ? 2 : 4)) pass_kernel(PassP
       if (MODE == kModeInit) {
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-          const uint4 w = P.X[r * (B / 4) + sub * NV + v];
+          const uint4 w = ld_block<COH>(P.X + r * (B / 4) + sub * NV + v);
           t[4 * v + 0] = w.x; t[4 * v + 1] = w.y; t[4 * v + 2] = w.z; t[4 * v + 3] = w.w;
         }
       } else {
@@ -472,7 +477,7 @@ __global__ void __launch_bounds__(kThreads, (B >= 32 ? 2 : 4)) pass_kernel(PassP
             h[l] = 0;
           }
         } else {
-          gather_sum<B, FE>(P.cv, P.rowptr[r], P.rowptr[r + 1], 1u, P.X, sub, M, acc);
+          gather_sum<B, FE, COH>(P.cv, P.rowptr[r], P.rowptr[r + 1], 1u, P.X, sub, M, acc);
         }
 #pragma unroll
         for (int l = 0; l < LPT; ++l) t[l] = redc(acc[l], M);  // t = (row sum) R^{-1}
@@ -588,6 +593,96 @@ __global__ void __launch_bounds__(kThreads, (B >= 32 ? 2 : 4)) pass_kernel(PassP
     if (P.term_ctr != nullptr && threadIdx.x == 0) *P.term_ctr += 1u;  // read above by thread 0 only after the barrier
   }
   if (threadIdx.x == 0) atomicExch(P.counter, 0u);
+}
+
+// Four CTAs (32 warps) per SM: the walk is latency bound, so occupancy is
+// worth a few spilled registers (measured on the 2M x 1.5M Zipf matrix).  At
+// B = 32 the Gram accumulators alone take 48 registers, and two CTAs per SM
+// with 128 registers run the same matrix 1.2x faster than four with spills.
+template <int B, int MODE, int FE>
+__global__ void __launch_bounds__(kThreads, (B >= 32 ? 2 : 4)) pass_kernel(PassParams P) {
+  extern __shared__ __align__(16) uint32_t gram_smem[];
+  __shared__ unsigned long long red[B * (B + 1) / 2];
+  __shared__ bool is_last;
+  pass_body<B, MODE, FE, false>(P, gram_smem, red, is_last);
+}
+
+// ---------------------------------------------------------------- persistent batched loop
+// Grid-wide barrier of a cooperative launch: thread 0 of each CTA arrives on
+// bar[0]; the last arrival resets it and advances the generation bar[1]; the
+// others wait for the generation to move, at most limit_ns of wall time
+// (%globaltimer), after which they set *error and every CTA returns false at
+// this or the next barrier.  `expected` is the number of CTAs that arrive.
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ bool grid_barrier(unsigned int* bar, int* error, uint64_t limit_ns, unsigned int expected) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    volatile unsigned int* gen = bar + 1;
+    const unsigned int g = *gen;
+    __threadfence();
+    if (atomicAdd(bar, 1u) == expected - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      const uint64_t t0 = global_ns();
+      while (*gen == g) {
+        if (*(volatile int*)error) { ok = 0; break; }
+        if (global_ns() - t0 > limit_ns) {
+          atomicExch(error, 1);
+          ok = 0;
+          break;
+        }
+        __nanosleep(128);
+      }
+    }
+    __threadfence();
+    s_ok = ok && *(volatile int*)error == 0;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// Applications [t_begin, t_end) of B for a batch phase in one launch: pass
+// over the stacked rows of A, grid barrier, pass over the rows of A^T, grid
+// barrier.  The blocks are read with coherent loads (they change between
+// barriers); the Gram partials go to the per-(matrix, term) slots.
+template <int B, int FE>
+__global__ void __launch_bounds__(kThreads, (B >= 32 ? 2 : 4)) persistent_kernel(PersistParams Q) {
+  extern __shared__ __align__(16) uint32_t gram_smem[];
+  __shared__ unsigned long long red[B * (B + 1) / 2];
+  __shared__ bool is_last;
+  int cur = Q.cur0;
+  for (int64_t t = Q.t_begin; t < Q.t_end; ++t) {
+    PassParams P = Q.odd;
+    P.X = Q.X[cur];
+    P.Y = Q.U;
+    P.term = 2 * t + 1;
+    pass_body<B, kModeOdd, FE, true>(P, gram_smem, red, is_last);
+    if (!grid_barrier(Q.bar, Q.error, Q.limit_ns, gridDim.x)) return;
+    P = Q.even;
+    P.X = Q.U;
+    P.Y = Q.X[cur ^ 1];
+    P.term = 2 * t + 2;
+    pass_body<B, kModeEven, FE, true>(P, gram_smem, red, is_last);
+    if (!grid_barrier(Q.bar, Q.error, Q.limit_ns, gridDim.x)) return;
+    cur ^= 1;
+  }
+}
+
+// A cooperative launch whose CTAs pass `rounds` grid barriers that wait for
+// `expected` arrivals (expected > gridDim.x: a barrier nothing completes).
+__global__ void barrier_check_kernel(unsigned int* bar, int* error, uint64_t limit_ns, unsigned int expected,
+                                     int rounds) {
+  for (int r = 0; r < rounds; ++r)
+    if (!grid_barrier(bar, error, limit_ns, expected)) return;
 }
 
 // Long rows: one warp per chunk of at most kChunkNnz entries.  Lanes form RPW
@@ -799,6 +894,56 @@ int launch_pass_raw(cudaStream_t s, int B, int fold4, int grid, const PassParams
     case 32: return launch_pass_raw_B<32>(s, fold4, grid, P, mode);
   }
   return fail(RR_EINVAL, "unsupported padded block width %d", B);
+}
+
+template <int B>
+static int launch_persistent_B(cudaStream_t s, int fold4, int grid, PersistParams& Q) {
+  const size_t sm = pass_smem_bytes<B>();
+  void* args[] = {&Q};
+  // the shared-memory limit was raised by persistent_blocks_per_sm at set-up
+  const void* fn = fold4 ? (const void*)persistent_kernel<B, 4> : (const void*)persistent_kernel<B, 2>;
+  RR_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kThreads), args, sm, s));
+  return RR_OK;
+}
+
+int launch_persistent_raw(cudaStream_t s, int B, int fold4, int grid, PersistParams& Q) {
+  switch (B) {
+    case 4: return launch_persistent_B<4>(s, fold4, grid, Q);
+    case 8: return launch_persistent_B<8>(s, fold4, grid, Q);
+    case 16: return launch_persistent_B<16>(s, fold4, grid, Q);
+    case 32: return launch_persistent_B<32>(s, fold4, grid, Q);
+  }
+  return fail(RR_EINVAL, "unsupported padded block width %d", B);
+}
+
+template <int B>
+static int persistent_blocks_B(int fold4, int* blocks) {
+  const size_t sm = pass_smem_bytes<B>();
+  if (fold4) {
+    RR_CUDA(cudaFuncSetAttribute(persistent_kernel<B, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, persistent_kernel<B, 4>, kThreads, sm));
+  } else {
+    RR_CUDA(cudaFuncSetAttribute(persistent_kernel<B, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, persistent_kernel<B, 2>, kThreads, sm));
+  }
+  return RR_OK;
+}
+
+int persistent_blocks_per_sm(int B, int fold4, int* blocks) {
+  switch (B) {
+    case 4: return persistent_blocks_B<4>(fold4, blocks);
+    case 8: return persistent_blocks_B<8>(fold4, blocks);
+    case 16: return persistent_blocks_B<16>(fold4, blocks);
+    case 32: return persistent_blocks_B<32>(fold4, blocks);
+  }
+  return fail(RR_EINVAL, "unsupported padded block width %d", B);
+}
+
+int launch_barrier_check(cudaStream_t s, int grid, unsigned int* bar, int* error, uint64_t limit_ns,
+                         unsigned int expected, int rounds) {
+  void* args[] = {&bar, &error, &limit_ns, &expected, &rounds};
+  RR_CUDA(cudaLaunchCooperativeKernel((const void*)barrier_check_kernel, dim3(grid), dim3(kThreads), args, 0, s));
+  return RR_OK;
 }
 
 template <int B>

@@ -61,6 +61,27 @@ struct ChunkParams {
   ModP M;
 };
 
+// The persistent batched loop (one cooperative launch per batch phase):
+// applications [t_begin, t_end), odd pass (rows of A: X[cur] -> U) then even
+// pass (rows of A^T: U -> X[cur ^ 1]) per application, separated by grid
+// barriers that give up after limit_ns and set *error.
+struct PersistParams {
+  PassParams odd, even;     // everything but X, Y and term
+  uint4* X[2];
+  uint4* U;
+  int cur0;
+  int64_t t_begin, t_end;
+  unsigned int* bar;        // [2]: arrivals, generation (zero before the first launch)
+  int* error;
+  uint64_t limit_ns;
+};
+int launch_persistent_raw(cudaStream_t s, int B, int fold4, int grid, PersistParams& Q);
+// Largest co-resident CTAs per SM of the persistent kernel (sets its shared-memory limit).
+int persistent_blocks_per_sm(int B, int fold4, int* blocks);
+// Cooperative launch of `grid` CTAs passing `rounds` barriers that wait for `expected` arrivals.
+int launch_barrier_check(cudaStream_t s, int grid, unsigned int* bar, int* error, uint64_t limit_ns,
+                         unsigned int expected, int rounds);
+
 // Finish the slot-per-term Gram sums of segments [seg_begin, seg_end):
 // S_all[seg_S_off[s] + t * pairs + q] = reduce(gram_all[seg_G_off[s] + t * NP + pair q]) * (t odd ? R : 1).
 int launch_batch_finalize(cudaStream_t s, const unsigned long long* gram_all, const int64_t* d_seg_G_off,

@@ -151,3 +151,60 @@ def test_batch_autotuner_shapes(ctx):
         ref, Lr, _ = oracle.krylov(rowptr, col, val, m, n, P, drs[i], dcs[i], vs[i], 0, L)
         assert np.array_equal(bt.sequence(i), ref[:, :Lr]), i
     bt.close()
+
+
+def test_batch_with_heavy_rows_and_columns(ctx):
+    """Matrices with rows and columns far above the chunking threshold (a dense
+    row, a dense column) in the batch: sequences equal the oracle's."""
+    b = 16
+    rng = np.random.default_rng(77)
+    mats = _mixed_batch(41, count=5)
+    m, n = 900, 700
+    rows = []
+    for r in range(m):
+        if r == 5:
+            c = np.arange(n)  # dense row of A (a heavy row of the stack)
+        else:
+            c = np.unique(np.concatenate([rng.choice(n, size=4), [11]]))  # column 11 dense: heavy row of A^T
+        rows.append(c)
+    rowptr = np.zeros(m + 1, np.int64)
+    rowptr[1:] = np.cumsum([len(c) for c in rows])
+    col = np.concatenate(rows).astype(np.int32)
+    val = rng.integers(1, P, size=col.size).astype(np.uint32)
+    mats.insert(2, (rowptr, col, val, m, n))
+    drs, dcs, vs = _inputs(mats, b, 17)
+    bt = rr.Batch(mats, b, P, drs, dcs, vs, ctx)
+    bt.krylov()
+    for i, (rowptr, col, val, m, n) in enumerate(mats):
+        L = rr.default_max_nlen(m, n, b)
+        ref, Lr, _ = oracle.krylov(rowptr, col, val, m, n, P, drs[i], dcs[i], vs[i], 0, L)
+        assert np.array_equal(bt.sequence(i), ref[:, :Lr]), i
+    bt.close()
+
+
+def test_grid_barrier_gives_up_and_context_survives(ctx):
+    """The persistent launch's grid barrier: with every CTA arriving it passes;
+    waiting for one CTA more than the grid has, every wait runs out after its
+    limit and reports it, and the context keeps working."""
+    import ctypes as C
+    import time
+
+    from rust_rank_b200 import _lib
+
+    t = C.c_int32(-1)
+    _lib.check(_lib.lib().rr_device_barrier_check(ctx.handle, 148, 148, 20, 1.0, C.byref(t)))
+    assert t.value == 0
+    t0 = time.perf_counter()
+    _lib.check(_lib.lib().rr_device_barrier_check(ctx.handle, 148, 149, 3, 0.3, C.byref(t)))
+    assert t.value == 1
+    assert time.perf_counter() - t0 < 10
+    # the context still runs work
+    b = 4
+    mats = _mixed_batch(5, count=3)
+    drs, dcs, vs = _inputs(mats, b, 3)
+    bt = rr.Batch(mats, b, P, drs, dcs, vs, ctx)
+    bt.krylov()
+    rowptr, col, val, m, n = mats[0]
+    ref, Lr, _ = oracle.krylov(rowptr, col, val, m, n, P, drs[0], dcs[0], vs[0], 0, rr.default_max_nlen(m, n, b))
+    assert np.array_equal(bt.sequence(0), ref[:, :Lr])
+    bt.close()
