@@ -146,6 +146,25 @@ __global__ void heavy_count_kernel(const uint32_t* __restrict__ deg, int64_t n, 
   if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
 }
 
+// pos[r * (P + 1) + j] = first entry of heavy row r whose column is >= j *
+// panel (j = 0..P; entries of a row are sorted by column).
+__global__ void panel_bounds_kernel(const uint2* __restrict__ cv, const uint32_t* __restrict__ ptr, int64_t heavy,
+                                    int P, uint32_t panel, uint32_t* __restrict__ pos) {
+  const int64_t total = heavy * (P + 1);
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = e / (P + 1);
+    const int j = (int)(e - r * (P + 1));
+    uint32_t lo = ptr[r], hi = ptr[r + 1];
+    const uint64_t key = (uint64_t)j * panel;
+    while (lo < hi) {
+      const uint32_t mid = lo + (hi - lo) / 2;
+      if ((uint64_t)cv[mid].x < key) lo = mid + 1;
+      else hi = mid;
+    }
+    pos[e] = lo;
+  }
+}
+
 __global__ void chunk_keys_kernel(const uint2* __restrict__ cv, const uint32_t* __restrict__ begin, int64_t nchunks,
                                   uint32_t* __restrict__ keys) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nchunks; i += (int64_t)gridDim.x * blockDim.x)
@@ -197,21 +216,50 @@ int degree_order_device(const uint32_t* deg, int64_t n, uint32_t maxd, DevBuf<in
 
 // Rows [0, heavy) of d are longer than kHeavyDegree: cut them into chunks of
 // at most kChunkNnz entries, ordered (stably) by their first column, so that
-// chunks gathering the same region of the input block run together.
+// chunks gathering the same region of the input block run together.  A row
+// whose chunks would each span more than one panel of kPanelCols columns of
+// the input block (rows of at least kChunkNnz entries per panel are dense
+// enough not to) is first cut at the panel boundaries, as long as its pieces
+// keep kMinPiece entries on average: the pieces of different rows that fall in
+// one panel then run together and gather from one L2-sized slice of the block.
+constexpr uint32_t kPanelCols = 1u << 18;
+constexpr int64_t kMinPiece = 64;
+
 int build_chunks(DevCsr& d, int64_t heavy, cudaStream_t s) {
   d.heavy_rows = heavy;
   d.nchunks = 0;
   if (heavy == 0) return RR_OK;
   std::vector<uint32_t> ptr(heavy + 1);
   RR_CUDA(cudaMemcpyAsync(ptr.data(), d.rowptr.ptr, (heavy + 1) * 4, cudaMemcpyDeviceToHost, s));
+  const int P = (int)std::max<int64_t>(1, (d.cols + kPanelCols - 1) / kPanelCols);
+  std::vector<uint32_t> pos;
+  if (P > 1) {
+    DevBuf<uint32_t> dpos;
+    RR_TRY(dpos.alloc_async((size_t)heavy * (P + 1), s));
+    panel_bounds_kernel<<<build_grid(heavy * (P + 1)), kBuildThreads, 0, s>>>(d.cv.ptr, d.rowptr.ptr, heavy, P,
+                                                                                 kPanelCols, dpos.ptr);
+    RR_CUDA(cudaGetLastError());
+    pos.resize((size_t)heavy * (P + 1));
+    RR_CUDA(cudaMemcpyAsync(pos.data(), dpos.ptr, pos.size() * 4, cudaMemcpyDeviceToHost, s));
+  }
   RR_CUDA(cudaStreamSynchronize(s));
   std::vector<uint32_t> row, beg, end;
-  for (int64_t r = 0; r < heavy; ++r)
-    for (uint32_t k = ptr[r]; k < ptr[r + 1]; k += (uint32_t)kChunkNnz) {
+  auto cut = [&](int64_t r, uint32_t a, uint32_t b) {
+    for (uint32_t k = a; k < b; k += (uint32_t)kChunkNnz) {
       row.push_back((uint32_t)r);
       beg.push_back(k);
-      end.push_back(std::min<uint32_t>(ptr[r + 1], k + (uint32_t)kChunkNnz));
+      end.push_back(std::min<uint32_t>(b, k + (uint32_t)kChunkNnz));
     }
+  };
+  for (int64_t r = 0; r < heavy; ++r) {
+    const int64_t deg = (int64_t)ptr[r + 1] - ptr[r];
+    if (P > 1 && deg >= kMinPiece * P && deg < (int64_t)kChunkNnz * P) {
+      const uint32_t* pr = pos.data() + (size_t)r * (P + 1);
+      for (int j = 0; j < P; ++j) cut(r, j == 0 ? ptr[r] : pr[j], j == P - 1 ? ptr[r + 1] : pr[j + 1]);
+    } else {
+      cut(r, ptr[r], ptr[r + 1]);
+    }
+  }
   const int64_t nc = (int64_t)row.size();
   DevBuf<uint32_t> dbeg, dkeys;
   RR_TRY(dbeg.alloc_async(nc, s));

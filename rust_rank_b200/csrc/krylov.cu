@@ -794,22 +794,40 @@ static int pass_grid(const rr_krylov* kr, int64_t rows) {
   return (int)std::max<int64_t>(1, std::min<int64_t>(kr->grid_pass, need));
 }
 
+// A launch with the handle's L2 access policy window (U persisting) as a
+// per-launch attribute: no stream state changes, and captured launches keep it.
+template <class... Args>
+static int launch_with_l2(const rr_krylov* kr, void (*fn)(Args...), dim3 grid, dim3 block, size_t smem,
+                          cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  if (kr->l2win.num_bytes > 0) {
+    attr[0].id = cudaLaunchAttributeAccessPolicyWindow;
+    attr[0].val.accessPolicyWindow = kr->l2win;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+  }
+  RR_CUDA(cudaLaunchKernelEx(&cfg, fn, args...));
+  return RR_OK;
+}
+
 template <int B>
 static int launch_pass_B(rr_krylov* kr, const PassParams& P, int mode) {
   const dim3 grid(pass_grid<B>(kr, P.rows)), block(kThreads);
   cudaStream_t s = kr->launch_stream ? kr->launch_stream : kr->mat->ctx->stream;
   const size_t sm = pass_smem_bytes<B>();
   if (kr->fold4) {
-    if (mode == kModeInit) pass_kernel<B, kModeInit, 4><<<grid, block, sm, s>>>(P);
-    else if (mode == kModeOdd) pass_kernel<B, kModeOdd, 4><<<grid, block, sm, s>>>(P);
-    else pass_kernel<B, kModeEven, 4><<<grid, block, sm, s>>>(P);
-  } else {
-    if (mode == kModeInit) pass_kernel<B, kModeInit, 2><<<grid, block, sm, s>>>(P);
-    else if (mode == kModeOdd) pass_kernel<B, kModeOdd, 2><<<grid, block, sm, s>>>(P);
-    else pass_kernel<B, kModeEven, 2><<<grid, block, sm, s>>>(P);
+    if (mode == kModeInit) return launch_with_l2(kr, pass_kernel<B, kModeInit, 4>, grid, block, sm, s, P);
+    if (mode == kModeOdd) return launch_with_l2(kr, pass_kernel<B, kModeOdd, 4>, grid, block, sm, s, P);
+    return launch_with_l2(kr, pass_kernel<B, kModeEven, 4>, grid, block, sm, s, P);
   }
-  RR_CUDA(cudaGetLastError());
-  return RR_OK;
+  if (mode == kModeInit) return launch_with_l2(kr, pass_kernel<B, kModeInit, 2>, grid, block, sm, s, P);
+  if (mode == kModeOdd) return launch_with_l2(kr, pass_kernel<B, kModeOdd, 2>, grid, block, sm, s, P);
+  return launch_with_l2(kr, pass_kernel<B, kModeEven, 2>, grid, block, sm, s, P);
 }
 
 template <int B, int FE>
@@ -837,10 +855,8 @@ static int launch_chunk_B(rr_krylov* kr, const ChunkParams& P) {
   const dim3 grid((unsigned)std::max<int64_t>(1, std::min<int64_t>(kr->grid_chunk, (P.nchunks + kWarps - 1) / kWarps))),
       block(kThreads);
   cudaStream_t s = kr->launch_stream ? kr->launch_stream : kr->mat->ctx->stream;
-  if (kr->fold4) chunk_kernel<B, 4><<<grid, block, 0, s>>>(P);
-  else chunk_kernel<B, 2><<<grid, block, 0, s>>>(P);
-  RR_CUDA(cudaGetLastError());
-  return RR_OK;
+  if (kr->fold4) return launch_with_l2(kr, chunk_kernel<B, 4>, grid, block, 0, s, P);
+  return launch_with_l2(kr, chunk_kernel<B, 2>, grid, block, 0, s, P);
 }
 
 static int launch_chunk(rr_krylov* kr, const ChunkParams& P) {
