@@ -390,7 +390,7 @@ __device__ __forceinline__ unsigned long long* seg_target(const PassParams& P, u
 // One pass over the rows of A (MODE odd), of A^T (even) or the initial
 // scaling (init), by the whole CTA: gram_smem is the per-warp Gram staging,
 // red[NP] the CTA's Gram reduction, is_last a shared flag.
-template <int B, int MODE, int FE, bool COH>
+template <int B, int MODE, int FE, bool COH, bool GRAM = true>
 __device__ __forceinline__ void pass_body(const PassParams& P, uint32_t* gram_smem, unsigned long long* red,
                                           bool& is_last) {
   using S = Shape<B>;
@@ -408,7 +408,7 @@ __device__ __forceinline__ void pass_body(const PassParams& P, uint32_t* gram_sm
 
   for (int q = threadIdx.x; q < NP; q += kThreads) red[q] = 0;
   Gram gram;
-  const bool emit = P.S_out != nullptr || P.term_ctr != nullptr;
+  const bool emit = GRAM && (P.S_out != nullptr || P.term_ctr != nullptr);
   if (emit) gram.init(gram_smem + (size_t)warp * Gram::kWords, lane);
   __syncthreads();  // red[] zeroed before a warp may emit into it
 
@@ -459,7 +459,7 @@ __device__ __forceinline__ void pass_body(const PassParams& P, uint32_t* gram_sm
     uint32_t gz[LPT], gu[LPT];
     if (r < P.rows) {
       uint32_t t[LPT];
-      if (MODE == kModeInit) {
+      if (MODE == kModeInit || MODE == kModeGram) {
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
           const uint4 w = ld_block<COH>(P.X + r * (B / 4) + sub * NV + v);
@@ -501,6 +501,14 @@ __device__ __forceinline__ void pass_body(const PassParams& P, uint32_t* gram_sm
           gu[l] = gz[l];
           o[l] = redc((uint64_t)gz[l] * s2, M);
         }
+      } else if (MODE == kModeGram) {
+        // gz = x * d^{-1} (scale = d^{-1} R); gu = gz or x
+#pragma unroll
+        for (int l = 0; l < LPT; ++l) {
+          gz[l] = redc((uint64_t)t[l] * s1, M);
+          gu[l] = P.gram_sym ? gz[l] : t[l];
+          o[l] = 0;
+        }
       } else {
         // init: w given; x = d_c w = redc(w * d_c R)
 #pragma unroll
@@ -510,9 +518,11 @@ __device__ __forceinline__ void pass_body(const PassParams& P, uint32_t* gram_sm
           o[l] = redc((uint64_t)t[l] * s1, M);
         }
       }
+      if (MODE != kModeGram) {
 #pragma unroll
-      for (int v = 0; v < NV; ++v)
-        P.Y[r * (B / 4) + sub * NV + v] = make_uint4(o[4 * v], o[4 * v + 1], o[4 * v + 2], o[4 * v + 3]);
+        for (int v = 0; v < NV; ++v)
+          P.Y[r * (B / 4) + sub * NV + v] = make_uint4(o[4 * v], o[4 * v + 1], o[4 * v + 2], o[4 * v + 3]);
+      }
     } else {
 #pragma unroll
       for (int l = 0; l < LPT; ++l) { gz[l] = 0; gu[l] = 0; }
@@ -599,12 +609,12 @@ __device__ __forceinline__ void pass_body(const PassParams& P, uint32_t* gram_sm
 // worth a few spilled registers (measured on the 2M x 1.5M Zipf matrix).  At
 // B = 32 the Gram accumulators alone take 48 registers, and two CTAs per SM
 // with 128 registers run the same matrix 1.2x faster than four with spills.
-template <int B, int MODE, int FE>
-__global__ void __launch_bounds__(kThreads, (B >= 32 ? 2 : 4)) pass_kernel(PassParams P) {
+template <int B, int MODE, int FE, bool GRAM = true>
+__global__ void __launch_bounds__(kThreads, (B >= 32 && GRAM ? 2 : 4)) pass_kernel(PassParams P) {
   extern __shared__ __align__(16) uint32_t gram_smem[];
   __shared__ unsigned long long red[B * (B + 1) / 2];
   __shared__ bool is_last;
-  pass_body<B, MODE, FE, false>(P, gram_smem, red, is_last);
+  pass_body<B, MODE, FE, false, GRAM>(P, gram_smem, red, is_last);
 }
 
 // ---------------------------------------------------------------- persistent batched loop
@@ -794,6 +804,13 @@ static int pass_grid(const rr_krylov* kr, int64_t rows) {
   return (int)std::max<int64_t>(1, std::min<int64_t>(kr->grid_pass, need));
 }
 
+template <int B>
+static int pass_grid_lean(const rr_krylov* kr, int64_t rows) {
+  const int64_t nbatch = (rows + Shape<B>::RPW - 1) / Shape<B>::RPW;
+  const int64_t need = (nbatch + kWarps - 1) / kWarps;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(kr->grid_lean, need));
+}
+
 // A launch with the handle's L2 access policy window (U persisting) as a
 // per-launch attribute: no stream state changes, and captured launches keep it.
 template <class... Args>
@@ -815,19 +832,28 @@ static int launch_with_l2(const rr_krylov* kr, void (*fn)(Args...), dim3 grid, d
   return RR_OK;
 }
 
+// Single-matrix launches: the odd and even passes run without their Gram
+// terms (no staging, no tensor-core flush, so fewer registers and no shared
+// memory), each followed by a Gram pass over the block it wrote (kModeGram);
+// the initial pass computes S_0 itself.
+template <int B, int FE>
+static int launch_pass_BF(rr_krylov* kr, const PassParams& P, int mode, dim3 grid, cudaStream_t s) {
+  const dim3 block(kThreads);
+  const size_t sm = pass_smem_bytes<B>();
+  switch (mode) {
+    case kModeInit: return launch_with_l2(kr, pass_kernel<B, kModeInit, FE, true>, grid, block, sm, s, P);
+    case kModeOdd: return launch_with_l2(kr, pass_kernel<B, kModeOdd, FE, false>, grid, block, 0, s, P);
+    case kModeEven: return launch_with_l2(kr, pass_kernel<B, kModeEven, FE, false>, grid, block, 0, s, P);
+    default: return launch_with_l2(kr, pass_kernel<B, kModeGram, FE, true>, grid, block, sm, s, P);
+  }
+}
+
 template <int B>
 static int launch_pass_B(rr_krylov* kr, const PassParams& P, int mode) {
-  const dim3 grid(pass_grid<B>(kr, P.rows)), block(kThreads);
+  const bool lean = mode == kModeOdd || mode == kModeEven;
+  const dim3 grid(lean ? pass_grid_lean<B>(kr, P.rows) : pass_grid<B>(kr, P.rows));
   cudaStream_t s = kr->launch_stream ? kr->launch_stream : kr->mat->ctx->stream;
-  const size_t sm = pass_smem_bytes<B>();
-  if (kr->fold4) {
-    if (mode == kModeInit) return launch_with_l2(kr, pass_kernel<B, kModeInit, 4>, grid, block, sm, s, P);
-    if (mode == kModeOdd) return launch_with_l2(kr, pass_kernel<B, kModeOdd, 4>, grid, block, sm, s, P);
-    return launch_with_l2(kr, pass_kernel<B, kModeEven, 4>, grid, block, sm, s, P);
-  }
-  if (mode == kModeInit) return launch_with_l2(kr, pass_kernel<B, kModeInit, 2>, grid, block, sm, s, P);
-  if (mode == kModeOdd) return launch_with_l2(kr, pass_kernel<B, kModeOdd, 2>, grid, block, sm, s, P);
-  return launch_with_l2(kr, pass_kernel<B, kModeEven, 2>, grid, block, sm, s, P);
+  return kr->fold4 ? launch_pass_BF<B, 4>(kr, P, mode, grid, s) : launch_pass_BF<B, 2>(kr, P, mode, grid, s);
 }
 
 template <int B, int FE>
@@ -836,6 +862,7 @@ static int set_pass_smem() {
   RR_CUDA(cudaFuncSetAttribute(pass_kernel<B, kModeInit, FE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
   RR_CUDA(cudaFuncSetAttribute(pass_kernel<B, kModeOdd, FE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
   RR_CUDA(cudaFuncSetAttribute(pass_kernel<B, kModeEven, FE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  RR_CUDA(cudaFuncSetAttribute(pass_kernel<B, kModeGram, FE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
   return RR_OK;
 }
 
@@ -871,16 +898,18 @@ static int launch_chunk(rr_krylov* kr, const ChunkParams& P) {
 }
 
 template <int B>
-static int occupancy_B(rr_krylov* kr, int* pass_blocks, int* chunk_blocks) {
+static int occupancy_B(rr_krylov* kr, int* pass_blocks, int* chunk_blocks, int* lean_blocks) {
   const size_t sm = pass_smem_bytes<B>();
   if (kr->fold4) {
     RR_TRY((set_pass_smem<B, 4>()));
-    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(pass_blocks, pass_kernel<B, kModeEven, 4>, kThreads, sm));
+    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(pass_blocks, pass_kernel<B, kModeGram, 4>, kThreads, sm));
     RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(chunk_blocks, chunk_kernel<B, 4>, kThreads, 0));
+    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(lean_blocks, pass_kernel<B, kModeOdd, 4, false>, kThreads, 0));
   } else {
     RR_TRY((set_pass_smem<B, 2>()));
-    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(pass_blocks, pass_kernel<B, kModeEven, 2>, kThreads, sm));
+    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(pass_blocks, pass_kernel<B, kModeGram, 2>, kThreads, sm));
     RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(chunk_blocks, chunk_kernel<B, 2>, kThreads, 0));
+    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(lean_blocks, pass_kernel<B, kModeOdd, 2, false>, kThreads, 0));
   }
   return RR_OK;
 }
@@ -996,17 +1025,18 @@ int rows_per_batch(int B) {
 }
 
 int krylov_occupancy(rr_krylov* kr) {
-  int pb = 1, cb = 1;
+  int pb = 1, cb = 1, lb = 1;
   switch (kr->B) {
-    case 4: RR_TRY(occupancy_B<4>(kr, &pb, &cb)); break;
-    case 8: RR_TRY(occupancy_B<8>(kr, &pb, &cb)); break;
-    case 16: RR_TRY(occupancy_B<16>(kr, &pb, &cb)); break;
-    case 32: RR_TRY(occupancy_B<32>(kr, &pb, &cb)); break;
+    case 4: RR_TRY(occupancy_B<4>(kr, &pb, &cb, &lb)); break;
+    case 8: RR_TRY(occupancy_B<8>(kr, &pb, &cb, &lb)); break;
+    case 16: RR_TRY(occupancy_B<16>(kr, &pb, &cb, &lb)); break;
+    case 32: RR_TRY(occupancy_B<32>(kr, &pb, &cb, &lb)); break;
     default: return fail(RR_EINVAL, "unsupported padded block width %d", kr->B);
   }
   const int sms = kr->mat->ctx->num_sms;
   kr->grid_pass = std::max(1, pb) * sms;
   kr->grid_chunk = std::max(1, cb) * sms;
+  kr->grid_lean = std::max(1, lb) * sms;
   return RR_OK;
 }
 
@@ -1072,11 +1102,18 @@ int krylov_launch_application(rr_krylov* kr, cudaEvent_t* ev) {
   P.X = reinterpret_cast<const uint4*>(x);
   P.Y = reinterpret_cast<uint4*>(kr->U.ptr);
   P.scale = kr->dr_m.ptr;
-  P.gram_mul = kr->M.r1;  // the odd Gram is accumulated from z R^{-1}
-  P.S_out = nullptr;  // slot len - base, from the device term counter
-  P.term_ctr = kr->d_term.ptr;
-  P.S_ptr = kr->d_sptr.ptr;
   RR_TRY(launch_pass(kr, P, kModeOdd));
+  // odd term: sum over rows of z (x) U with z = U d_r^{-1}
+  {
+    PassParams G = base_params(kr);
+    G.rows = mat->A.rows;
+    G.X = reinterpret_cast<const uint4*>(kr->U.ptr);
+    G.scale = kr->drinv_r.ptr;
+    G.gram_sym = 0;
+    G.term_ctr = kr->d_term.ptr;
+    G.S_ptr = kr->d_sptr.ptr;
+    RR_TRY(launch_pass(kr, G, kModeGram));
+  }
   if (ev) RR_CUDA(cudaEventRecord(ev[1], s));
   // pass 2: rows of A^T
   RR_TRY(run_chunks(kr, mat->At, kr->U.ptr));
@@ -1089,8 +1126,18 @@ int krylov_launch_application(rr_krylov* kr, cudaEvent_t* ev) {
   P.Y = reinterpret_cast<uint4*>(xn);
   P.scale = kr->dc_m.ptr;
   P.scale2 = kr->dc_r.ptr;
-  P.gram_mul = 1;  // slot len + 1 - base
   RR_TRY(launch_pass(kr, P, kModeEven));
+  // even term: sum over rows of w' (x) w' with w' = x' d_c^{-1}
+  {
+    PassParams G = base_params(kr);
+    G.rows = mat->At.rows;
+    G.X = reinterpret_cast<const uint4*>(xn);
+    G.scale = kr->dcinv_r.ptr;
+    G.gram_sym = 1;
+    G.term_ctr = kr->d_term.ptr;
+    G.S_ptr = kr->d_sptr.ptr;
+    RR_TRY(launch_pass(kr, G, kModeGram));
+  }
   if (ev) RR_CUDA(cudaEventRecord(ev[3], s));
   kr->len += 2;
   kr->cur ^= 1;
@@ -1110,24 +1157,33 @@ int krylov_launch_get_curv(rr_krylov* kr, uint32_t* d_out) {
 
 // The preconditioners in device order and in the forms the epilogues use:
 // d_r R^2, d_c R^2, d_c R and d_c^{-1} (mod p; the inverse by Fermat, p prime).
+__device__ __forceinline__ uint32_t inverse_mod(uint32_t a, const ModP& M) {  // a^(p-2), p prime
+  uint32_t r = 1;
+  for (uint32_t e = M.p - 2; e; e >>= 1) {
+    if (e & 1) r = mulmod(r, a, M);
+    a = mulmod(a, a, M);
+  }
+  return r;
+}
+
 __global__ void precond_kernel(const uint32_t* __restrict__ rp, const uint32_t* __restrict__ cp,
                                const int32_t* __restrict__ rowperm, const int32_t* __restrict__ colperm, int64_t m,
                                int64_t n, uint32_t R1, uint32_t R2, ModP M, uint32_t* __restrict__ dr_m,
-                               uint32_t* __restrict__ dc_m, uint32_t* __restrict__ dc_r, uint32_t* __restrict__ dcinv) {
+                               uint32_t* __restrict__ drinv_r, uint32_t* __restrict__ dc_m, uint32_t* __restrict__ dc_r,
+                               uint32_t* __restrict__ dcinv, uint32_t* __restrict__ dcinv_r) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m + n; i += (int64_t)gridDim.x * blockDim.x) {
     if (i < m) {
-      dr_m[i] = mulmod(rp[rowperm[i]], R2, M);
+      const uint32_t r = rp[rowperm[i]];
+      dr_m[i] = mulmod(r, R2, M);
+      drinv_r[i] = mulmod(inverse_mod(r, M), R1, M);
     } else {
       const int64_t j = i - m;
       const uint32_t c = cp[colperm[j]];
       dc_m[j] = mulmod(c, R2, M);
       dc_r[j] = mulmod(c, R1, M);
-      uint32_t r = 1, a = c;
-      for (uint32_t e = M.p - 2; e; e >>= 1) {
-        if (e & 1) r = mulmod(r, a, M);
-        a = mulmod(a, a, M);
-      }
-      dcinv[j] = r;
+      const uint32_t ci = inverse_mod(c, M);
+      dcinv[j] = ci;
+      dcinv_r[j] = mulmod(ci, R1, M);
     }
   }
 }
@@ -1139,7 +1195,8 @@ int launch_precond(rr_krylov* kr, const uint32_t* d_rp, const uint32_t* d_cp, co
   const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((m + n + threads - 1) / threads, 4 * 148 * 8));
   precond_kernel<<<blocks, threads, 0, kr->mat->ctx->stream>>>(d_rp, d_cp, d_rowperm, kr->mat->d_colperm.ptr, m, n,
                                                                (uint32_t)R1, (uint32_t)R2, kr->M, kr->dr_m.ptr,
-                                                               kr->dc_m.ptr, kr->dc_r.ptr, kr->dcinv.ptr);
+                                                               kr->drinv_r.ptr, kr->dc_m.ptr, kr->dc_r.ptr,
+                                                               kr->dcinv.ptr, kr->dcinv_r.ptr);
   RR_CUDA(cudaGetLastError());
   return RR_OK;
 }

@@ -5,7 +5,10 @@
 
 namespace rr {
 
-enum PassMode { kModeInit = 0, kModeOdd = 1, kModeEven = 2 };
+// kModeGram: no output block; the Gram term of the rows of X with
+// gz = redc(x * scale) and gu = gram_sym ? gz : x (a Gram pass after a pass
+// that did not compute its term).
+enum PassMode { kModeInit = 0, kModeOdd = 1, kModeEven = 2, kModeGram = 3 };
 
 struct PassParams {
   const uint32_t* rowptr;
@@ -36,6 +39,7 @@ struct PassParams {
   uint32_t gram_mul;        // factor applied to the finished term
   uint32_t w4, w5, w6;      // 2^32, 2^40, 2^48 mod p (limb weights of the tensor-core Gram)
   int b_real;
+  int gram_sym;             // kModeGram: both Gram factors scaled
   ModP M;
   // Batched mode (many matrices stacked block-diagonally, each padded to a
   // multiple of 32 rows): batch_seg[batch] is the matrix of a row batch.  Warps

@@ -165,8 +165,9 @@ struct rr_krylov_s {
   rr::ModP M{};
   int fold4 = 0;  // 1 when four products fit between folds
   // preconditioners in device order, in the forms the epilogues use:
-  // d_r R^2, d_c R^2, d_c R (mod p, R = 2^32) and d_c^{-1}
-  rr::DevBuf<uint32_t> dr_m, dc_m, dc_r, dcinv;
+  // d_r R^2, d_c R^2, d_c R (mod p, R = 2^32), d_c^{-1}, and the Gram passes'
+  // d_r^{-1} R and d_c^{-1} R
+  rr::DevBuf<uint32_t> dr_m, dc_m, dc_r, dcinv, drinv_r, dcinv_r;
   rr::DevBuf<uint32_t> X[2];           // x_k = D_c w_k, n x B interleaved
   rr::DevBuf<uint32_t> U;              // D_r A x_k, m x B
   rr::DevBuf<unsigned long long> heavy_acc;
@@ -177,7 +178,7 @@ struct rr_krylov_s {
   int64_t base = 0; // first term held in S
   int64_t len = 0;  // terms queued so far
   int cur = 0;      // index of the current X
-  int grid_pass = 0, grid_chunk = 0;
+  int grid_pass = 0, grid_chunk = 0, grid_lean = 0;
   int64_t launches = 0;  // kernels launched by this handle
   // device-indexed sequence output: next slot (len - base) and the S pointer
   rr::DevBuf<unsigned int> d_term;
