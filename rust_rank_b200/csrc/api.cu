@@ -314,6 +314,8 @@ int rr_krylov_create(rr_matrix* mat, int32_t b, const uint32_t* row_precond, con
   RR_CUDA(cudaMemsetAsync(kr->heavy_acc.ptr, 0, kr->heavy_acc.bytes(), s));
   RR_TRY(kr->gram_acc.alloc_async((size_t)kGramReplicas * (B * (B + 1) / 2), s));
   RR_CUDA(cudaMemsetAsync(kr->gram_acc.ptr, 0, kr->gram_acc.bytes(), s));
+  RR_TRY(kr->d_status.alloc_async(1, s));
+  RR_CUDA(cudaMemsetAsync(kr->d_status.ptr, 0, sizeof(int), s));
   RR_TRY(kr->counter.alloc_async(4, s));
   RR_CUDA(cudaMemsetAsync(kr->counter.ptr, 0, kr->counter.bytes(), s));
   RR_TRY(kr->d_term.alloc_async(1, s));
@@ -431,9 +433,12 @@ int rr_krylov_fetch(rr_krylov* kr, int64_t from, int64_t to, uint32_t* seq, int6
   const int64_t cnt = to - from;
   if (cnt == 0) return RR_OK;
   std::vector<uint32_t> tmp((size_t)cnt * np);
+  int dstat = 0;
   RR_CUDA(cudaMemcpyAsync(tmp.data(), kr->S.ptr + (size_t)(from - kr->base) * np, tmp.size() * 4,
                           cudaMemcpyDeviceToHost, kr->mat->ctx->stream));
+  RR_CUDA(cudaMemcpyAsync(&dstat, kr->d_status.ptr, sizeof(int), cudaMemcpyDeviceToHost, kr->mat->ctx->stream));
   RR_CUDA(cudaStreamSynchronize(kr->mat->ctx->stream));
+  if (dstat) return fail(RR_ETIMEOUT, "a device-side wait of the Gram pass gave up; the terms are not valid");
   for (int64_t t = 0; t < cnt; ++t)
     for (int q = 0; q < np; ++q) seq[(size_t)q * seq_stride + from + t] = tmp[(size_t)t * np + q];
   return RR_OK;

@@ -617,6 +617,303 @@ __global__ void __launch_bounds__(kThreads, (B >= 32 && GRAM ? 2 : 4)) pass_kern
   pass_body<B, MODE, FE, false, GRAM>(P, gram_smem, red, is_last);
 }
 
+// ---------------------------------------------------------------- Gram pass on tcgen05
+// The Gram term of a block (kModeGram: gz = x * scale, gu = gram_sym ? gz : x
+// per row) on the 5th-generation tensor cores, for padded widths 16 and 32.
+//
+// Exact integers by byte limbs: with gz = sum_a 256^a Z_a and gu = sum_c 256^c
+// U_c (bytes), G[i][j] = sum_{a,c} 256^{a+c} (Z_a^T U_c)[i][j].  One UMMA
+// D[M x N] += A[M x K] B[N x K]^T (kind::i8, unsigned bytes, s32 accumulators
+// in TMEM) computes all 16 limb pairs at once: A row (a, i) holds limb a of
+// lane i of the tile's rows (K = rows), B row (c, j) limb c of gu; M = 128
+// (4 B rows, zero-padded to 128 for B = 16), N = 4 B.  A CTA stages 128-row
+// tiles into double-buffered shared memory in the canonical K-major layout
+// without swizzle (8-row x 16-byte core matrices; K-adjacent cores 128 bytes
+// apart, 8-row groups 256 bytes apart), one thread issues the four K = 32
+// MMAs of a tile and commits them to the buffer's mbarrier.  A per-row limb
+// product is < 2^16, so the int32 accumulators are drained into registers
+// every kTcDrain tiles.  At the end the four warps read D out of TMEM
+// (tcgen05.ld), weight limb pairs by 2^{8(a+c)} mod p, and the CTA's sums join
+// the same replicated 64-bit accumulators and last-CTA finish as the pass
+// kernels.  Every wait on an mbarrier gives up after 2 s and sets *status.
+constexpr int kTcRows = 128;        // rows (K bytes) per tile
+constexpr int kTcDrain = 64;        // tiles between drains of the int32 accumulators
+constexpr uint64_t kTcWaitLimitNs = 2000000000ull;  // 2 s of %globaltimer
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// K-major, no swizzle: start >> 4, LBO = 128 B (K-direction core stride),
+// SBO = 256 B (8-row group stride), descriptor version 1 (sm_100).
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(256 >> 4) << 32) |
+         (1ull << 46);
+}
+
+// Byte offset of (row, k) in a staged operand of R rows x 128 K-bytes.
+__device__ __forceinline__ uint32_t tc_off(int R, int row, int k) {
+  return (uint32_t)((k >> 5) * (R / 8) * 256 + (row >> 3) * 256 + ((k & 31) >> 4) * 128 + (row & 7) * 16 + (k & 15));
+}
+
+__device__ __forceinline__ uint64_t tc_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity) {
+  const uint64_t t0 = tc_ns();
+  for (;;) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(done)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (tc_ns() - t0 > kTcWaitLimitNs) return false;
+  }
+}
+
+template <int B>
+struct TcShape {
+  static constexpr int MR = 4 * B;              // real A rows (limb, lane)
+  static constexpr int M = 128;                 // UMMA M (zero rows above MR)
+  static constexpr int N = 4 * B;               // UMMA N
+  static constexpr int A_BYTES = M * kTcRows;   // per buffer
+  static constexpr int B_BYTES = N * kTcRows;
+  static constexpr int COLS = N <= 64 ? 64 : 128;  // TMEM columns allocated
+  static constexpr uint32_t IDESC = (2u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+};
+
+template <int B>
+constexpr size_t gram_tc_smem_bytes() {
+  return 2 * (size_t)(TcShape<B>::A_BYTES + TcShape<B>::B_BYTES);
+}
+
+template <int B>
+__global__ void __launch_bounds__(kThreads, 2) gram_tc_kernel(PassParams P, int* status) {
+  using T = TcShape<B>;
+  constexpr int NP = B * (B + 1) / 2;
+  extern __shared__ __align__(1024) unsigned char tc_smem[];
+  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ uint32_t tmem_base_s;
+  __shared__ unsigned long long red[B * B];
+  __shared__ bool is_last;
+  __shared__ int s_fail;
+  // buffer s: A at tc_smem + s (A + B bytes), B right after it
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const ModP M = P.M;
+
+  // zero both buffers once (the A rows above 4B stay zero), the CTA sums, the barriers
+  for (int e = tid; e < (int)(gram_tc_smem_bytes<B>() / 16); e += kThreads)
+    reinterpret_cast<uint4*>(tc_smem)[e] = make_uint4(0, 0, 0, 0);
+  for (int e = tid; e < B * B; e += kThreads) red[e] = 0;
+  if (tid == 0) {
+    s_fail = 0;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])) : "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)),
+                 "r"(T::COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base_s;
+
+  // per-thread sums of the drained limb products: thread (warp w < 4, lane l)
+  // owns A row m = 32 w + l = (a, i) and keeps sum_c 256^{a+c} D[m][(c, j)] mod p per j
+  uint32_t part[B];
+#pragma unroll
+  for (int j = 0; j < B; ++j) part[j] = 0;
+  const int m_row = 32 * warp + lane;
+  const bool reader = warp < 4 && m_row < T::MR;
+  const int a_limb = m_row / B;
+  uint32_t wgt[4];  // 2^{8(a + c)} mod p for c = 0..3
+  {
+    uint64_t w = 1;
+    for (int e = 0; e < (reader ? a_limb : 0); ++e) w = w * 256 % M.p;
+    for (int c = 0; c < 4; ++c) {
+      wgt[c] = (uint32_t)w;
+      w = w * 256 % M.p;
+    }
+  }
+  // drain: wait for every committed MMA, add D into part[], restart accumulation
+  uint32_t commits[2] = {0, 0};
+  auto drain = [&]() {
+    if (tid == 0) {
+      for (int s = 0; s < 2; ++s)
+        if (commits[s] && !mbar_wait(smem_u32(&mbar[s]), (commits[s] - 1) & 1)) {
+          s_fail = 1;
+          atomicExch(status, 1);
+        }
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (warp < 4) {
+#pragma unroll
+      for (int c0 = 0; c0 < T::N; c0 += 16) {
+        uint32_t v[16];
+        const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0;
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+            : "r"(taddr)
+            : "memory");
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (reader) {
+#pragma unroll
+          for (int q = 0; q < 16; ++q) {
+            const int n = c0 + q, c = n / B, j = n % B;
+            part[j] = addmod(part[j], mulmod(v[q], wgt[c], M), M.p);
+          }
+        }
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+  };
+
+  const int64_t ntiles = (P.rows + kTcRows - 1) / kTcRows;
+  int64_t tl = 0;        // tiles of this CTA so far
+  bool acc_live = false;  // D holds sums to accumulate onto
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++tl) {
+    const int s = (int)(tl & 1);
+    unsigned char* const bufA = tc_smem + s * (T::A_BYTES + T::B_BYTES);
+    unsigned char* const bufB = bufA + T::A_BYTES;
+    if (tl >= 2) {  // the MMAs of tile tl - 2 read this buffer
+      if (tid == 0 && !mbar_wait(smem_u32(&mbar[s]), (commits[s] - 1) & 1)) {
+        s_fail = 1;
+        atomicExch(status, 1);
+      }
+      __syncthreads();
+    }
+    if (s_fail) break;
+    // stage: 32 row-quads x B lanes; 4 rows of one lane become one word per limb
+    const int64_t r0 = tile * kTcRows;
+    for (int task = tid; task < 32 * B; task += kThreads) {
+      const int i = task % B, qd = task / B;
+      uint32_t z[4], u[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int64_t r = r0 + 4 * qd + q;
+        uint32_t y = 0, sc = 0;
+        if (r < P.rows) {
+          y = __ldg(reinterpret_cast<const uint32_t*>(P.X) + r * B + i);
+          sc = __ldg(P.scale + r);
+        }
+        z[q] = redc((uint64_t)y * sc, M);
+        u[q] = P.gram_sym ? z[q] : y;
+      }
+      uint32_t wz[4], wu[4];
+      {
+        const uint32_t t0 = __byte_perm(z[0], z[1], 0x5140), t1 = __byte_perm(z[2], z[3], 0x5140);
+        const uint32_t t2 = __byte_perm(z[0], z[1], 0x7362), t3 = __byte_perm(z[2], z[3], 0x7362);
+        wz[0] = __byte_perm(t0, t1, 0x5410);
+        wz[1] = __byte_perm(t0, t1, 0x7632);
+        wz[2] = __byte_perm(t2, t3, 0x5410);
+        wz[3] = __byte_perm(t2, t3, 0x7632);
+      }
+      {
+        const uint32_t t0 = __byte_perm(u[0], u[1], 0x5140), t1 = __byte_perm(u[2], u[3], 0x5140);
+        const uint32_t t2 = __byte_perm(u[0], u[1], 0x7362), t3 = __byte_perm(u[2], u[3], 0x7362);
+        wu[0] = __byte_perm(t0, t1, 0x5410);
+        wu[1] = __byte_perm(t0, t1, 0x7632);
+        wu[2] = __byte_perm(t2, t3, 0x5410);
+        wu[3] = __byte_perm(t2, t3, 0x7632);
+      }
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        *reinterpret_cast<uint32_t*>(bufA + tc_off(T::M, a * B + i, 4 * qd)) = wz[a];
+        *reinterpret_cast<uint32_t*>(bufB + tc_off(T::N, a * B + i, 4 * qd)) = wu[a];
+      }
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a0 = smem_u32(bufA), b0 = smem_u32(bufB);
+#pragma unroll
+      for (int kb = 0; kb < 4; ++kb) {
+        const uint64_t da = umma_desc(a0 + kb * (T::M / 8) * 256);
+        const uint64_t db = umma_desc(b0 + kb * (T::N / 8) * 256);
+        const uint32_t accum = (acc_live || kb > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+            :
+            : "r"(tmem), "l"(da), "l"(db), "r"(T::IDESC), "r"(accum), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+            : "memory");
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_u32(&mbar[s]))
+                   : "memory");
+    }
+    commits[s] += 1;
+    acc_live = true;
+    if ((tl + 1) % kTcDrain == 0) {
+      drain();
+      acc_live = false;
+    }
+  }
+  if (acc_live && !s_fail) drain();
+  if (s_fail) {  // let what was committed finish before the memory goes away
+    if (tid == 0)
+      for (int s = 0; s < 2; ++s)
+        if (commits[s]) mbar_wait(smem_u32(&mbar[s]), (commits[s] - 1) & 1);
+    __syncthreads();
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(T::COLS) : "memory");
+  }
+  // CTA sums: G[i][j] += part (4 limb rows a per (i, j))
+  if (reader) {
+    const int i = m_row % B;
+#pragma unroll
+    for (int j = 0; j < B; ++j) atomicAdd(&red[i * B + j], (unsigned long long)part[j]);
+  }
+  __syncthreads();
+  unsigned long long* const acc = P.gram_acc + (size_t)(blockIdx.x % P.replicas) * P.gram_stride;
+  for (int q = tid; q < NP; q += kThreads) {
+    int i, j;
+    pair_of(q, B, i, j);
+    atomicAdd(&acc[q], (unsigned long long)reduce(red[i * B + j], M));
+  }
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) is_last = (atomicAdd(P.counter, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!is_last) return;
+  __threadfence();
+  // the last CTA: the finished term (real pairs), then reset
+  const int b = P.b_real;
+  const int npr = b * (b + 1) / 2;
+  uint32_t* S_out = *P.S_ptr + (size_t)__ldcg(P.term_ctr) * npr;
+  for (int q = tid; q < npr; q += kThreads) {
+    int i, j;
+    pair_of(q, b, i, j);
+    const int qb = pair_index(i, j, B);
+    unsigned long long v = 0;
+    for (int r = 0; r < P.replicas; ++r) v += __ldcg(P.gram_acc + (size_t)r * P.gram_stride + qb);
+    S_out[q] = mulmod(reduce(v, M), P.gram_mul, M);
+  }
+  __syncthreads();
+  for (int q = tid; q < NP * P.replicas; q += kThreads)
+    __stcg(P.gram_acc + (size_t)(q / NP) * P.gram_stride + q % NP, 0ull);
+  if (tid == 0) {
+    *P.term_ctr += 1u;
+    atomicExch(P.counter, 0u);
+  }
+}
+
 // ---------------------------------------------------------------- persistent batched loop
 // Grid-wide barrier of a cooperative launch: thread 0 of each CTA arrives on
 // bar[0]; the last arrival resets it and advances the generation bar[1]; the
@@ -848,8 +1145,21 @@ static int launch_pass_BF(rr_krylov* kr, const PassParams& P, int mode, dim3 gri
   }
 }
 
+// Gram passes at padded widths 16 and 32 run on tcgen05 (gram_tc_kernel).
+template <int B>
+static int launch_gram_tc(rr_krylov* kr, const PassParams& P, cudaStream_t s) {
+  const int64_t ntiles = (P.rows + kTcRows - 1) / kTcRows;
+  const dim3 grid((unsigned)std::max<int64_t>(1, std::min<int64_t>(ntiles, 2 * (int64_t)kr->mat->ctx->num_sms)));
+  return launch_with_l2(kr, gram_tc_kernel<B>, grid, dim3(kThreads), gram_tc_smem_bytes<B>(), s, P,
+                        kr->d_status.ptr);
+}
+
 template <int B>
 static int launch_pass_B(rr_krylov* kr, const PassParams& P, int mode) {
+  if (mode == kModeGram && (B == 16 || B == 32)) {
+    cudaStream_t s = kr->launch_stream ? kr->launch_stream : kr->mat->ctx->stream;
+    return launch_gram_tc<(B >= 16 ? B : 16)>(kr, P, s);
+  }
   const bool lean = mode == kModeOdd || mode == kModeEven;
   const dim3 grid(lean ? pass_grid_lean<B>(kr, P.rows) : pass_grid<B>(kr, P.rows));
   cudaStream_t s = kr->launch_stream ? kr->launch_stream : kr->mat->ctx->stream;
@@ -1025,6 +1335,12 @@ int rows_per_batch(int B) {
 }
 
 int krylov_occupancy(rr_krylov* kr) {
+  if (kr->B == 16)
+    RR_CUDA(cudaFuncSetAttribute(gram_tc_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)gram_tc_smem_bytes<16>()));
+  if (kr->B == 32)
+    RR_CUDA(cudaFuncSetAttribute(gram_tc_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)gram_tc_smem_bytes<32>()));
   int pb = 1, cb = 1, lb = 1;
   switch (kr->B) {
     case 4: RR_TRY(occupancy_B<4>(kr, &pb, &cb, &lb)); break;

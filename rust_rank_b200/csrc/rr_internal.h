@@ -179,6 +179,7 @@ struct rr_krylov_s {
   int64_t len = 0;  // terms queued so far
   int cur = 0;      // index of the current X
   int grid_pass = 0, grid_chunk = 0, grid_lean = 0;
+  rr::DevBuf<int> d_status;  // set by a device-side wait that gave up (tcgen05 Gram pass)
   int64_t launches = 0;  // kernels launched by this handle
   // device-indexed sequence output: next slot (len - base) and the S pointer
   rr::DevBuf<unsigned int> d_term;
