@@ -45,12 +45,22 @@ constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 static_assert(kWarps == kPassWarps, "host-side run tables assume this many warps per CTA");
 
+// Threads of a warp split into RPW row slots of TPR threads; a thread owns
+// LPT lanes of its row's block, as NV 128-bit words interleaved with the other
+// threads of the slot: word v of thread `sub` is word v * TPR + sub of the row
+// (lanes 4 (v TPR + sub) .. + 3).  So one warp load instruction reads TPR
+// adjacent 16-byte words per row -- whole 32-byte sectors for B >= 8 -- and a
+// gathered row costs the L1 the minimum of B / 8 sector accesses.
 template <int B>
 struct Shape {
-  static constexpr int LPT = (B >= 8) ? 8 : 4;  // lanes of the block per thread
-  static constexpr int NV = LPT / 4;             // 128-bit words per thread per row
-  static constexpr int TPR = B / LPT;            // threads per row
-  static constexpr int RPW = 32 / TPR;           // rows per warp batch (slots)
+  static constexpr int LPT = (B >= 16) ? 8 : 4;  // lanes of the block per thread
+  static constexpr int NV = LPT / 4;              // 128-bit words per thread per row
+  static constexpr int TPR = B / LPT;             // threads per row
+  static constexpr int RPW = 32 / TPR;            // rows per warp batch (slots)
+  // block lane of this thread's lane l
+  static __device__ __forceinline__ int lane_of(int sub, int l) { return 4 * ((l >> 2) * TPR + sub) + (l & 3); }
+  // 128-bit word index within a row of this thread's word v
+  static __device__ __forceinline__ int word_of(int sub, int v) { return v * TPR + sub; }
 };
 
 __device__ __forceinline__ void pair_of(int q, int B, int& i, int& j) {
@@ -107,7 +117,7 @@ __device__ __forceinline__ void gather_sum(const uint2* __restrict__ cv, uint32_
                                            uint64_t (&acc)[Shape<B>::LPT]) {
   constexpr int NV = Shape<B>::NV;
   constexpr int RW = B / 4;  // 128-bit words per block row
-  const uint4* Xs = X + sub * NV;
+  const uint4* Xs = X + sub;  // word v of the row at Xs + v * TPR
   uint32_t k = beg;
   const uint32_t step = 4 * stride;
   if (k + 3 * stride < end) {
@@ -119,7 +129,7 @@ __device__ __forceinline__ void gather_sum(const uint2* __restrict__ cv, uint32_
 #pragma unroll
       for (int u = 0; u < 4; ++u)
 #pragma unroll
-        for (int v = 0; v < NV; ++v) g[u][v] = ld_block<COH>(Xs + (size_t)e[u].x * RW + v);
+        for (int v = 0; v < NV; ++v) g[u][v] = ld_block<COH>(Xs + (size_t)e[u].x * RW + v * Shape<B>::TPR);
       k += step;
       const bool more = k + 3 * stride < end;
       uint2 en[4];
@@ -145,7 +155,7 @@ __device__ __forceinline__ void gather_sum(const uint2* __restrict__ cv, uint32_
 #pragma unroll
     for (int u = 0; u < 4; ++u)
 #pragma unroll
-      for (int v = 0; v < NV; ++v) g[u][v] = ld_block<COH>(Xs + (size_t)e[u].x * RW + v);
+      for (int v = 0; v < NV; ++v) g[u][v] = ld_block<COH>(Xs + (size_t)e[u].x * RW + v * Shape<B>::TPR);
     mac_step<B, FE>(e, g, M, acc);
   }
 }
@@ -184,8 +194,8 @@ struct GramCore {
                                       int lane, const ModP& M, const uint32_t (&)[3]) {
 #pragma unroll
     for (int l = 0; l < LPT; ++l) {
-      zs[slot * B + LPT * sub + l] = gz[l];
-      us[slot * B + LPT * sub + l] = gu[l];
+      zs[slot * B + Shape<B>::lane_of(sub, l)] = gz[l];
+      us[slot * B + Shape<B>::lane_of(sub, l)] = gu[l];
     }
     __syncwarp();
 #pragma unroll
@@ -278,7 +288,7 @@ struct GramMma {
     const int word = (bt * RPW + (slot & ~3)) >> 2;  // 4-row group inside the K tile
 #pragma unroll
     for (int l = 0; l < LPT; ++l) {
-      const int i = LPT * sub + l;
+      const int i = Shape<B>::lane_of(sub, l);
       pz[(rho * BM + i) * RS + word] = transpose4(gz[l], rho);
       pu[(rho * BM + i) * RS + word] = transpose4(gu[l], rho);
     }
@@ -462,7 +472,7 @@ __device__ __forceinline__ void pass_body(const PassParams& P, uint32_t* gram_sm
       if (MODE == kModeInit || MODE == kModeGram) {
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-          const uint4 w = ld_block<COH>(P.X + r * (B / 4) + sub * NV + v);
+          const uint4 w = ld_block<COH>(P.X + r * (B / 4) + S::word_of(sub, v));
           t[4 * v + 0] = w.x; t[4 * v + 1] = w.y; t[4 * v + 2] = w.z; t[4 * v + 3] = w.w;
         }
       } else {
@@ -470,11 +480,11 @@ __device__ __forceinline__ void pass_body(const PassParams& P, uint32_t* gram_sm
 #pragma unroll
         for (int l = 0; l < LPT; ++l) acc[l] = 0;
         if (r < P.heavy_rows) {
-          unsigned long long* h = P.heavy_acc + (size_t)r * B + LPT * sub;
+          unsigned long long* h = P.heavy_acc + (size_t)r * B;
 #pragma unroll
           for (int l = 0; l < LPT; ++l) {
-            acc[l] = fold(h[l], M);
-            h[l] = 0;
+            acc[l] = fold(h[S::lane_of(sub, l)], M);
+            h[S::lane_of(sub, l)] = 0;
           }
         } else {
           gather_sum<B, FE, COH>(P.cv, P.rowptr[r], P.rowptr[r + 1], 1u, P.X, sub, M, acc);
@@ -521,7 +531,7 @@ __device__ __forceinline__ void pass_body(const PassParams& P, uint32_t* gram_sm
       if (MODE != kModeGram) {
 #pragma unroll
         for (int v = 0; v < NV; ++v)
-          P.Y[r * (B / 4) + sub * NV + v] = make_uint4(o[4 * v], o[4 * v + 1], o[4 * v + 2], o[4 * v + 3]);
+          P.Y[r * (B / 4) + S::word_of(sub, v)] = make_uint4(o[4 * v], o[4 * v + 1], o[4 * v + 2], o[4 * v + 3]);
       }
     } else {
 #pragma unroll
@@ -1022,9 +1032,9 @@ __global__ void __launch_bounds__(kThreads, 3) chunk_kernel(ChunkParams P) {
       for (int l = 0; l < LPT; ++l) y[l] = addmod(y[l], __shfl_xor_sync(0xffffffffu, y[l], off), M.p);
     }
     if (slot == 0) {
-      unsigned long long* h = P.heavy_acc + (size_t)row * B + LPT * sub;
+      unsigned long long* h = P.heavy_acc + (size_t)row * B;
 #pragma unroll
-      for (int l = 0; l < LPT; ++l) atomicAdd(&h[l], (unsigned long long)y[l]);
+      for (int l = 0; l < LPT; ++l) atomicAdd(&h[S::lane_of(sub, l)], (unsigned long long)y[l]);
     }
   }
 }
