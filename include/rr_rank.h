@@ -231,10 +231,16 @@ int rr_batch_ranks(rr_batch* batch, int32_t workers, int64_t* ranks);
 /* Launch shapes the batch's autotuner picked: the Krylov loop has one phase
  * per distinct set of running matrices (phase k covers applications
  * apps_from[k] .. apps_from[k+1]-1); ctas[k] is the grid of its persistent
- * launch, chosen at create time by timing 1..(co-resident maximum) CTAs per
- * SM.  Call with NULL arrays to get the phase count; *nphases gives the room
- * of the arrays. */
+ * launch, chosen at create time together with the block shape
+ * (rr_batch_tuning_shape) by timing every shape with 1..(co-resident maximum)
+ * CTAs per SM.  Call with NULL arrays to get the phase count; *nphases gives
+ * the room of the arrays. */
 int rr_batch_tuning(const rr_batch* batch, int32_t* nphases, int32_t* ctas, int64_t* apps_from);
+/* The block shape the autotuner picked per phase (beside its grid, see
+ * rr_batch_tuning): lanes of the block each thread owns (4 or 8) and, from
+ * it, the rows a warp walks together (32 * lanes / padded width).  Call with
+ * NULL arrays to get the phase count. */
+int rr_batch_tuning_shape(const rr_batch* batch, int32_t* nphases, int32_t* lanes_per_thread, int32_t* rows_per_warp);
 /* Stacked sizes: rows and columns with padding, nonzeros, applications of
  * B of the longest sequence. */
 int rr_batch_info(const rr_batch* batch, int64_t* total_rows, int64_t* total_cols, int64_t* total_nnz,

@@ -484,6 +484,15 @@ class Batch:
         check(lib().rr_batch_tuning(self.handle, C.byref(k), ptr(ctas), ptr(first)))
         return [(int(a), int(c)) for a, c in zip(first, ctas)]
 
+    def tuning_shape(self):
+        """[(lanes per thread, rows per warp batch)] per phase, as the autotuner chose them."""
+        k = C.c_int32(0)
+        check(lib().rr_batch_tuning_shape(self.handle, C.byref(k), None, None))
+        lanes = np.zeros(k.value, np.int32)
+        rows = np.zeros(k.value, np.int32)
+        check(lib().rr_batch_tuning_shape(self.handle, C.byref(k), ptr(lanes), ptr(rows)))
+        return [(int(a), int(b)) for a, b in zip(lanes, rows)]
+
     def info(self):
         r, c, z, a = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()
         check(lib().rr_batch_info(self.handle, C.byref(r), C.byref(c), C.byref(z), C.byref(a)))

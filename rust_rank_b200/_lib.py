@@ -63,6 +63,7 @@ SIGNATURES = {
     "rr_batch_ranks": (C.c_int, [_vp, _i32, _vp]),
     "rr_batch_info": (C.c_int, [_vp, _pi64, _pi64, _pi64, _pi64]),
     "rr_batch_tuning": (C.c_int, [_vp, _pi32, _vp, _vp]),
+    "rr_batch_tuning_shape": (C.c_int, [_vp, _pi32, _vp, _vp]),
     "rr_device_barrier_check": (C.c_int, [_vp, _i32, _i32, _i32, C.c_double, _pi32]),
     "rr_wdm_save": (C.c_int, [C.c_char_p, _i64, _i64, _u32, _i32, _vp, _vp, _vp, _vp, _vp, _i64, _i64]),
     "rr_wdm_load": (C.c_int, [C.c_char_p, _pi64, _pi64, _pu32, _pi32, _pi64, _vp, _vp, _vp, _vp, _vp, _i64]),

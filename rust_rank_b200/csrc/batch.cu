@@ -48,7 +48,16 @@ struct rr_batch_s {
   std::vector<int64_t> row_off, col_off;  // padded offsets per stack position (+1 entries)
   std::vector<int64_t> s_off;    // sequence offset (words) per stack position
   rr::DevCsr A, At;
-  rr::DevBuf<int32_t> seg_rows, seg_cols;  // matrix of each row batch of A / A^T
+  // lanes-per-thread variants of the persistent kernel (rows per warp batch
+  // differ): per variant, the matrix of each row batch of A / A^T and the
+  // work prefix over row batches; variant kDefaultVariant is also the shape
+  // of the initial pass
+  int nvar = 1;
+  int lpt[2] = {4, 4};
+  rr::DevBuf<int32_t> seg_rows[2], seg_cols[2];
+  std::vector<int64_t> work_rows[2], work_cols[2];
+  int def_var = 0;
+  std::vector<int> phase_var;    // phase -> lanes-per-thread variant (autotuned)
   // equal-work warp runs per phase (a phase = a set of running matrices):
   // runs_*[phase][warp], kPassWarps * grid + 1 entries each
   rr::DevBuf<int32_t> runs_rows, runs_cols;
@@ -153,11 +162,10 @@ std::vector<int64_t> batch_work(const std::vector<uint32_t>& ptr, int rpb) {
 }
 
 // Warp-run tables (both passes) of phase ph for a grid of `grid` CTAs.
-void phase_runs(const rr_batch* bt, int ph, int grid, const std::vector<int64_t>& wa, const std::vector<int64_t>& wt,
-                int32_t* ra, int32_t* rt) {
-  const int rpb = rows_per_batch(bt->B), f = bt->phase_first[ph], nw = grid * kPassWarps;
-  equal_runs(wa, bt->row_off[f] / rpb, bt->row_off[bt->nmat] / rpb, nw, ra);
-  equal_runs(wt, bt->col_off[f] / rpb, bt->col_off[bt->nmat] / rpb, nw, rt);
+void phase_runs(const rr_batch* bt, int ph, int grid, int var, int32_t* ra, int32_t* rt) {
+  const int rpb = rows_per_batch(bt->B, bt->lpt[var]), f = bt->phase_first[ph], nw = grid * kPassWarps;
+  equal_runs(bt->work_rows[var], bt->row_off[f] / rpb, bt->row_off[bt->nmat] / rpb, nw, ra);
+  equal_runs(bt->work_cols[var], bt->col_off[f] / rpb, bt->col_off[bt->nmat] / rpb, nw, rt);
 }
 
 // A grid-wide barrier wait gives up after this long (the whole phase then
@@ -166,9 +174,9 @@ constexpr uint64_t kBarrierLimitNs = 2000000000ull;
 
 // Parameters of the persistent launch of phase ph for applications
 // [t_begin, t_end) with the given grid and warp-run tables.
-PersistParams phase_params(rr_batch* bt, int ph, const int32_t* d_ra, const int32_t* d_rt, int64_t t_begin,
+PersistParams phase_params(rr_batch* bt, int ph, int var, const int32_t* d_ra, const int32_t* d_rt, int64_t t_begin,
                            int64_t t_end, int cur0) {
-  const int rpb = rows_per_batch(bt->B), nmat = bt->nmat, first = bt->phase_first[ph];
+  const int rpb = rows_per_batch(bt->B, bt->lpt[var]), nmat = bt->nmat, first = bt->phase_first[ph];
   PersistParams Q;
   std::memset(&Q, 0, sizeof(Q));
   PassParams P = batch_params(bt);
@@ -181,7 +189,7 @@ PersistParams phase_params(rr_batch* bt, int ph, const int32_t* d_ra, const int3
   P.rows = bt->row_off[nmat];
   P.scale = bt->dr_m.ptr;
   P.gram_mul = bt->M.r1;
-  P.batch_seg = bt->seg_rows.ptr;
+  P.batch_seg = bt->seg_rows[var].ptr;
   P.runs = d_ra;
   P.batch_begin = bt->row_off[first] / rpb;
   Q.odd = P;
@@ -192,7 +200,7 @@ PersistParams phase_params(rr_batch* bt, int ph, const int32_t* d_ra, const int3
   P.scale = bt->dc_m.ptr;
   P.scale2 = bt->dc_r.ptr;
   P.gram_mul = 1;
-  P.batch_seg = bt->seg_cols.ptr;
+  P.batch_seg = bt->seg_cols[var].ptr;
   P.runs = d_rt;
   P.batch_begin = bt->col_off[first] / rpb;
   Q.even = P;
@@ -208,11 +216,11 @@ PersistParams phase_params(rr_batch* bt, int ph, const int32_t* d_ra, const int3
   return Q;
 }
 
-int launch_phase(rr_batch* bt, int ph, int grid, const int32_t* d_ra, const int32_t* d_rt, int64_t t_begin,
+int launch_phase(rr_batch* bt, int ph, int var, int grid, const int32_t* d_ra, const int32_t* d_rt, int64_t t_begin,
                  int64_t t_end, int cur0) {
-  PersistParams Q = phase_params(bt, ph, d_ra, d_rt, t_begin, t_end, cur0);
+  PersistParams Q = phase_params(bt, ph, var, d_ra, d_rt, t_begin, t_end, cur0);
   RR_CUDA(cudaMemsetAsync(bt->bar.ptr, 0, 2 * sizeof(unsigned int), bt->stream));
-  return launch_persistent_raw(bt->stream, bt->B, bt->fold4, grid, Q);
+  return launch_persistent_raw(bt->stream, bt->B, bt->fold4, grid, bt->lpt[var], Q);
 }
 
 // Autotuner: for every phase, time a persistent launch of three
@@ -223,9 +231,11 @@ int launch_phase(rr_batch* bt, int ph, int grid, const int32_t* d_ra, const int3
 // The timed applications write terms 1..6 of the running matrices and
 // scratch blocks only; the slots are cleared and the Krylov loop recomputes
 // all of them.
-int tune_phases(rr_batch* bt, int max_cps, const std::vector<int64_t>& wa, const std::vector<int64_t>& wt) {
+int tune_phases(rr_batch* bt, const int* max_cps) {
   const int nph = (int)bt->phase_first.size(), sms = bt->ctx->num_sms;
-  const int max_grid = std::max(1, max_cps) * sms;
+  int cps_top = 1;
+  for (int v = 0; v < bt->nvar; ++v) cps_top = std::max(cps_top, max_cps[v]);
+  const int max_grid = cps_top * sms;
   RR_CUDA(cudaMemsetAsync(bt->X[0].ptr, 0, bt->X[0].bytes(), bt->stream));
   RR_CUDA(cudaMemsetAsync(bt->X[1].ptr, 0, bt->X[1].bytes(), bt->stream));
   RR_CUDA(cudaMemsetAsync(bt->U.ptr, 0, bt->U.bytes(), bt->stream));
@@ -237,44 +247,47 @@ int tune_phases(rr_batch* bt, int max_cps, const std::vector<int64_t>& wa, const
   RR_CUDA(cudaEventCreate(&e0));
   RR_CUDA(cudaEventCreate(&e1));
   int status = RR_OK;
-  bt->phase_grid.assign(nph, max_grid);
+  bt->phase_grid.assign(nph, sms);
+  bt->phase_var.assign(nph, bt->def_var);
   for (int ph = 0; ph < nph && status == RR_OK; ++ph) {
-    float best = 0.f;
-    for (int cps = 1; cps <= std::max(1, max_cps) && status == RR_OK; ++cps) {
-      const int grid = cps * sms;
-      phase_runs(bt, ph, grid, wa, wt, ra.data(), rt.data());
-      const size_t words = (size_t)grid * kPassWarps + 1;
-      if (cudaMemcpyAsync(dra.ptr, ra.data(), words * 4, cudaMemcpyHostToDevice, bt->stream) != cudaSuccess ||
-          cudaMemcpyAsync(drt.ptr, rt.data(), words * 4, cudaMemcpyHostToDevice, bt->stream) != cudaSuccess) {
-        status = fail(RR_ECUDA, "tuning upload failed");
-        break;
+    float best = -1.f;
+    for (int var = 0; var < bt->nvar && status == RR_OK; ++var)
+      for (int cps = 1; cps <= std::max(1, max_cps[var]) && status == RR_OK; ++cps) {
+        const int grid = cps * sms;
+        phase_runs(bt, ph, grid, var, ra.data(), rt.data());
+        const size_t words = (size_t)grid * kPassWarps + 1;
+        if (cudaMemcpyAsync(dra.ptr, ra.data(), words * 4, cudaMemcpyHostToDevice, bt->stream) != cudaSuccess ||
+            cudaMemcpyAsync(drt.ptr, rt.data(), words * 4, cudaMemcpyHostToDevice, bt->stream) != cudaSuccess) {
+          status = fail(RR_ECUDA, "tuning upload failed");
+          break;
+        }
+        status = launch_phase(bt, ph, var, grid, dra.ptr, drt.ptr, 0, 1, 0);  // warm-up
+        if (status == RR_OK) cudaEventRecord(e0, bt->stream);
+        if (status == RR_OK) status = launch_phase(bt, ph, var, grid, dra.ptr, drt.ptr, 0, 3, 0);
+        if (status != RR_OK) break;
+        cudaEventRecord(e1, bt->stream);
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+          status = fail(RR_ECUDA, "tuning: %s", cudaGetErrorString(cudaGetLastError()));
+          break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (best < 0.f || ms < best) {
+          best = ms;
+          bt->phase_grid[ph] = grid;
+          bt->phase_var[ph] = var;
+        }
       }
-      status = launch_phase(bt, ph, grid, dra.ptr, drt.ptr, 0, 1, 0);  // warm-up
-      if (status == RR_OK) cudaEventRecord(e0, bt->stream);
-      if (status == RR_OK) status = launch_phase(bt, ph, grid, dra.ptr, drt.ptr, 0, 3, 0);
-      if (status != RR_OK) break;
-      cudaEventRecord(e1, bt->stream);
-      if (cudaEventSynchronize(e1) != cudaSuccess) {
-        status = fail(RR_ECUDA, "tuning: %s", cudaGetErrorString(cudaGetLastError()));
-        break;
-      }
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, e0, e1);
-      if (cps == 1 || ms < best) {
-        best = ms;
-        bt->phase_grid[ph] = grid;
-      }
-    }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (status != RR_OK) return status;
-  // final tables with the chosen grids
+  // final tables with the chosen shapes
   bt->run_off.assign(nph + 1, 0);
   for (int ph = 0; ph < nph; ++ph) bt->run_off[ph + 1] = bt->run_off[ph] + (int64_t)bt->phase_grid[ph] * kPassWarps + 1;
   std::vector<int32_t> fa(bt->run_off[nph]), ft(bt->run_off[nph]);
   for (int ph = 0; ph < nph; ++ph)
-    phase_runs(bt, ph, bt->phase_grid[ph], wa, wt, fa.data() + bt->run_off[ph], ft.data() + bt->run_off[ph]);
+    phase_runs(bt, ph, bt->phase_grid[ph], bt->phase_var[ph], fa.data() + bt->run_off[ph], ft.data() + bt->run_off[ph]);
   RR_TRY(bt->runs_rows.alloc(fa.size()));
   RR_TRY(bt->runs_cols.alloc(ft.size()));
   RR_CUDA(cudaMemcpyAsync(bt->runs_rows.ptr, fa.data(), fa.size() * 4, cudaMemcpyHostToDevice, bt->stream));
@@ -305,7 +318,7 @@ int krylov_queue(rr_batch* bt, cudaEvent_t* ev) {
     P.X = reinterpret_cast<const uint4*>(bt->W0.ptr);
     P.Y = reinterpret_cast<uint4*>(bt->X[0].ptr);
     P.scale = bt->dc_r.ptr;
-    P.batch_seg = bt->seg_cols.ptr;
+    P.batch_seg = bt->seg_cols[bt->def_var].ptr;
     P.batch_begin = 0;
     P.seg_begin = 0;
     P.seg_end = nmat;
@@ -321,8 +334,8 @@ int krylov_queue(rr_batch* bt, cudaEvent_t* ev) {
     const int ph = bt->phase_of[first];
     const int64_t t_end = bt->apps[first];  // the next sequence end
     const size_t run_off = (size_t)bt->run_off[ph];
-    RR_TRY(launch_phase(bt, ph, bt->phase_grid[ph], bt->runs_rows.ptr + run_off, bt->runs_cols.ptr + run_off, t, t_end,
-                        cur));
+    RR_TRY(launch_phase(bt, ph, bt->phase_var[ph], bt->phase_grid[ph], bt->runs_rows.ptr + run_off,
+                        bt->runs_cols.ptr + run_off, t, t_end, cur));
     cur ^= (int)((t_end - t) & 1);
     t = t_end;
     // matrices whose sequences end here: finish their terms
@@ -513,12 +526,23 @@ int rr_batch_create(rr_ctx* ctx, int32_t nmat, const int64_t* m, const int64_t* 
   });
   aptr[Mtot] = (uint32_t)nnz;
   tptr[Ntot] = (uint32_t)nnz;
-  // segment of every row batch
-  const int rpb = rows_per_batch(bt->B);
-  std::vector<int32_t> srow(Mtot / rpb), scol(Ntot / rpb);
-  for (int s = 0; s < nmat; ++s) {
-    for (int64_t q = bt->row_off[s] / rpb; q < bt->row_off[s + 1] / rpb; ++q) srow[q] = s;
-    for (int64_t q = bt->col_off[s] / rpb; q < bt->col_off[s + 1] / rpb; ++q) scol[q] = s;
+  // lanes-per-thread variants; the segment of every row batch and the work
+  // prefix over row batches for each
+  bt->nvar = persistent_lane_options(bt->B, bt->lpt);
+  bt->def_var = 0;
+  for (int v = 0; v < bt->nvar; ++v)
+    if (rows_per_batch(bt->B, bt->lpt[v]) == rows_per_batch(bt->B)) bt->def_var = v;
+  std::vector<int32_t> srow[2], scol[2];
+  for (int v = 0; v < bt->nvar; ++v) {
+    const int rpb = rows_per_batch(bt->B, bt->lpt[v]);
+    srow[v].resize(Mtot / rpb);
+    scol[v].resize(Ntot / rpb);
+    for (int s = 0; s < nmat; ++s) {
+      for (int64_t q = bt->row_off[s] / rpb; q < bt->row_off[s + 1] / rpb; ++q) srow[v][q] = s;
+      for (int64_t q = bt->col_off[s] / rpb; q < bt->col_off[s + 1] / rpb; ++q) scol[v][q] = s;
+    }
+    bt->work_rows[v] = batch_work(aptr, rpb);
+    bt->work_cols[v] = batch_work(tptr, rpb);
   }
   cudaStream_t st = ctx->stream;
   auto up = [&](auto& buf, const auto& vec) -> int {
@@ -533,8 +557,10 @@ int rr_batch_create(rr_ctx* ctx, int32_t nmat, const int64_t* m, const int64_t* 
   RR_TRY(up(bt->A.cv, acv));
   RR_TRY(up(bt->At.rowptr, tptr));
   RR_TRY(up(bt->At.cv, tcv));
-  RR_TRY(up(bt->seg_rows, srow));
-  RR_TRY(up(bt->seg_cols, scol));
+  for (int v = 0; v < bt->nvar; ++v) {
+    RR_TRY(up(bt->seg_rows[v], srow[v]));
+    RR_TRY(up(bt->seg_cols[v], scol[v]));
+  }
   RR_TRY(up(bt->dr_m, drm));
   RR_TRY(up(bt->dc_m, dcm));
   RR_TRY(up(bt->dc_r, dcr));
@@ -563,9 +589,9 @@ int rr_batch_create(rr_ctx* ctx, int32_t nmat, const int64_t* m, const int64_t* 
   RR_TRY(bt->error.alloc(1));
   RR_CUDA(cudaMemsetAsync(bt->bar.ptr, 0, bt->bar.bytes(), st));
   RR_CUDA(cudaMemsetAsync(bt->error.ptr, 0, bt->error.bytes(), st));
-  int blocks = 1, pblocks = 1;
+  int blocks = 1, pblocks[2] = {1, 1};
   RR_TRY(pass_blocks_per_sm(bt->B, bt->fold4, &blocks));
-  RR_TRY(persistent_blocks_per_sm(bt->B, bt->fold4, &pblocks));
+  for (int v = 0; v < bt->nvar; ++v) RR_TRY(persistent_blocks_per_sm(bt->B, bt->fold4, bt->lpt[v], &pblocks[v]));
   bt->grid = std::max(1, blocks) * ctx->num_sms;
   // phases: one per distinct set of running matrices
   bt->phase_of.assign(nmat, -1);
@@ -574,12 +600,11 @@ int rr_batch_create(rr_ctx* ctx, int32_t nmat, const int64_t* m, const int64_t* 
       bt->phase_of[s] = (int)bt->phase_first.size();
       bt->phase_first.push_back(s);
     }
-  const std::vector<int64_t> wa = batch_work(aptr, rpb), wt = batch_work(tptr, rpb);
   int prio_lo = 0, prio_hi = 0;
   RR_CUDA(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
   RR_CUDA(cudaStreamCreateWithPriority(&bt->stream, cudaStreamNonBlocking, prio_hi));
   RR_CUDA(cudaStreamSynchronize(st));
-  RR_TRY(tune_phases(bt.get(), std::max(1, pblocks), wa, wt));
+  RR_TRY(tune_phases(bt.get(), pblocks));
   RR_TRY(krylov_status(bt.get()));
   RR_CUDA(cudaMemsetAsync(bt->gram_all.ptr, 0, bt->gram_all.bytes(), bt->stream));
   RR_CUDA(cudaStreamSynchronize(bt->stream));
@@ -767,6 +792,21 @@ int rr_batch_ranks(rr_batch* bt, int32_t workers, int64_t* ranks) {
   if (krc != RR_OK) return fail(krc, "%s", kerr.c_str());
   for (int w = 0; w < workers; ++w)
     if (status[w] != RR_OK) return fail(status[w], "generator worker %d: %s", w, errors[w].c_str());
+  return RR_OK;
+}
+
+int rr_batch_tuning_shape(const rr_batch* bt, int32_t* nphases, int32_t* lanes_per_thread, int32_t* rows_per_warp) {
+  if (!bt || !nphases) return fail(RR_EINVAL, "NULL argument");
+  const int nph = (int)bt->phase_first.size();
+  if (lanes_per_thread || rows_per_warp) {
+    if (*nphases < nph) return fail(RR_EINVAL, "room for %d phases, %d needed", *nphases, nph);
+    for (int ph = 0; ph < nph; ++ph) {
+      const int l = bt->lpt[bt->phase_var[ph]];
+      if (lanes_per_thread) lanes_per_thread[ph] = l;
+      if (rows_per_warp) rows_per_warp[ph] = rows_per_batch(bt->B, l);
+    }
+  }
+  *nphases = nph;
   return RR_OK;
 }
 

@@ -52,8 +52,11 @@ static_assert(kWarps == kPassWarps, "host-side run tables assume this many warps
 // adjacent 16-byte words per row -- whole 32-byte sectors for B >= 8 -- and a
 // gathered row costs the L1 the minimum of B / 8 sector accesses.
 template <int B>
+constexpr int kDefaultLpt = (B >= 16) ? 8 : 4;
+
+template <int B, int L = kDefaultLpt<B>>
 struct Shape {
-  static constexpr int LPT = (B >= 16) ? 8 : 4;  // lanes of the block per thread
+  static constexpr int LPT = L;                   // lanes of the block per thread
   static constexpr int NV = LPT / 4;              // 128-bit words per thread per row
   static constexpr int TPR = B / LPT;             // threads per row
   static constexpr int RPW = 32 / TPR;            // rows per warp batch (slots)
@@ -78,14 +81,14 @@ __device__ __forceinline__ void pair_of(int q, int B, int& i, int& j) {
 // for this thread's LPT lanes (lane block `sub`).  Four entries per step, all
 // loads issued before the multiplies; acc is folded after every FE products,
 // so it leaves folded (< p * 2^32).
-template <int B, int FE>
-__device__ __forceinline__ void mac_step(const uint2 (&e)[4], const uint4 (&g)[4][Shape<B>::NV], const ModP& M,
-                                         uint64_t (&acc)[Shape<B>::LPT]) {
+template <int B, int FE, int L = kDefaultLpt<B>>
+__device__ __forceinline__ void mac_step(const uint2 (&e)[4], const uint4 (&g)[4][Shape<B, L>::NV], const ModP& M,
+                                         uint64_t (&acc)[Shape<B, L>::LPT]) {
 #pragma unroll
   for (int u = 0; u < 4; ++u) {
     const uint32_t val = e[u].y;
 #pragma unroll
-    for (int v = 0; v < Shape<B>::NV; ++v) {
+    for (int v = 0; v < Shape<B, L>::NV; ++v) {
       acc[4 * v + 0] = mad_wide(val, g[u][v].x, acc[4 * v + 0]);
       acc[4 * v + 1] = mad_wide(val, g[u][v].y, acc[4 * v + 1]);
       acc[4 * v + 2] = mad_wide(val, g[u][v].z, acc[4 * v + 2]);
@@ -93,7 +96,7 @@ __device__ __forceinline__ void mac_step(const uint2 (&e)[4], const uint4 (&g)[4
     }
     if ((u % FE) == FE - 1) {
 #pragma unroll
-      for (int l = 0; l < Shape<B>::LPT; ++l) acc[l] = fold(acc[l], M);
+      for (int l = 0; l < Shape<B, L>::LPT; ++l) acc[l] = fold(acc[l], M);
     }
   }
 }
@@ -111,11 +114,11 @@ __device__ __forceinline__ uint4 ld_block(const uint4* p) {
   return __ldg(p);
 }
 
-template <int B, int FE, bool COH = false>
+template <int B, int FE, bool COH = false, int L = kDefaultLpt<B>>
 __device__ __forceinline__ void gather_sum(const uint2* __restrict__ cv, uint32_t beg, uint32_t end, uint32_t stride,
                                            const uint4* __restrict__ X, int sub, const ModP& M,
-                                           uint64_t (&acc)[Shape<B>::LPT]) {
-  constexpr int NV = Shape<B>::NV;
+                                           uint64_t (&acc)[Shape<B, L>::LPT]) {
+  constexpr int NV = Shape<B, L>::NV;
   constexpr int RW = B / 4;  // 128-bit words per block row
   const uint4* Xs = X + sub;  // word v of the row at Xs + v * TPR
   uint32_t k = beg;
@@ -129,7 +132,7 @@ __device__ __forceinline__ void gather_sum(const uint2* __restrict__ cv, uint32_
 #pragma unroll
       for (int u = 0; u < 4; ++u)
 #pragma unroll
-        for (int v = 0; v < NV; ++v) g[u][v] = ld_block<COH>(Xs + (size_t)e[u].x * RW + v * Shape<B>::TPR);
+        for (int v = 0; v < NV; ++v) g[u][v] = ld_block<COH>(Xs + (size_t)e[u].x * RW + v * Shape<B, L>::TPR);
       k += step;
       const bool more = k + 3 * stride < end;
       uint2 en[4];
@@ -137,7 +140,7 @@ __device__ __forceinline__ void gather_sum(const uint2* __restrict__ cv, uint32_
 #pragma unroll
         for (int u = 0; u < 4; ++u) en[u] = __ldg(cv + k + u * stride);
       }
-      mac_step<B, FE>(e, g, M, acc);
+      mac_step<B, FE, L>(e, g, M, acc);
       if (!more) break;
 #pragma unroll
       for (int u = 0; u < 4; ++u) e[u] = en[u];
@@ -155,8 +158,8 @@ __device__ __forceinline__ void gather_sum(const uint2* __restrict__ cv, uint32_
 #pragma unroll
     for (int u = 0; u < 4; ++u)
 #pragma unroll
-      for (int v = 0; v < NV; ++v) g[u][v] = ld_block<COH>(Xs + (size_t)e[u].x * RW + v * Shape<B>::TPR);
-    mac_step<B, FE>(e, g, M, acc);
+      for (int v = 0; v < NV; ++v) g[u][v] = ld_block<COH>(Xs + (size_t)e[u].x * RW + v * Shape<B, L>::TPR);
+    mac_step<B, FE, L>(e, g, M, acc);
   }
 }
 
@@ -168,9 +171,9 @@ __device__ __forceinline__ int pair_index(int i, int j, int B) { return i * B - 
 
 // CUDA cores (B = 4): the batch is staged in shared memory and every lane
 // accumulates a few (i, j) pairs over the staged rows.
-template <int B, int FE>
+template <int B, int FE, int L = kDefaultLpt<B>>
 struct GramCore {
-  static constexpr int LPT = Shape<B>::LPT, RPW = Shape<B>::RPW;
+  static constexpr int LPT = Shape<B, L>::LPT, RPW = Shape<B, L>::RPW;
   static constexpr int NP = B * (B + 1) / 2, PPL = (NP + 31) / 32;
   static constexpr int kWords = 2 * RPW * B;  // shared words per warp
   uint32_t* zs;  // [RPW][B]
@@ -194,8 +197,8 @@ struct GramCore {
                                       int lane, const ModP& M, const uint32_t (&)[3]) {
 #pragma unroll
     for (int l = 0; l < LPT; ++l) {
-      zs[slot * B + Shape<B>::lane_of(sub, l)] = gz[l];
-      us[slot * B + Shape<B>::lane_of(sub, l)] = gu[l];
+      zs[slot * B + Shape<B, L>::lane_of(sub, l)] = gz[l];
+      us[slot * B + Shape<B, L>::lane_of(sub, l)] = gu[l];
     }
     __syncwarp();
 #pragma unroll
@@ -245,9 +248,9 @@ __device__ __forceinline__ void mma_u8(int (&d)[4], const uint32_t (&a)[4], uint
 // pair's product is < 32 * 255^2 < 2^21, so the shift classes s = a + c stay
 // exact in int32; classes 0..3 are recombined exactly in 64 bits (< 2^48) and
 // classes 4..6 are added with their weights 2^{8s} mod p.
-template <int B, int FE>
+template <int B, int FE, int L = kDefaultLpt<B>>
 struct GramMma {
-  static constexpr int LPT = Shape<B>::LPT, TPR = Shape<B>::TPR, RPW = Shape<B>::RPW;
+  static constexpr int LPT = Shape<B, L>::LPT, TPR = Shape<B, L>::TPR, RPW = Shape<B, L>::RPW;
   static constexpr int TB = 32 / RPW;           // batches per K tile
   static constexpr int BM = B < 16 ? 16 : B;    // rows of the M dimension (zero padded)
   static constexpr int MT = BM / 16, NT = B / 8;
@@ -288,7 +291,7 @@ struct GramMma {
     const int word = (bt * RPW + (slot & ~3)) >> 2;  // 4-row group inside the K tile
 #pragma unroll
     for (int l = 0; l < LPT; ++l) {
-      const int i = Shape<B>::lane_of(sub, l);
+      const int i = Shape<B, L>::lane_of(sub, l);
       pz[(rho * BM + i) * RS + word] = transpose4(gz[l], rho);
       pu[(rho * BM + i) * RS + word] = transpose4(gu[l], rho);
     }
@@ -400,14 +403,14 @@ __device__ __forceinline__ unsigned long long* seg_target(const PassParams& P, u
 // One pass over the rows of A (MODE odd), of A^T (even) or the initial
 // scaling (init), by the whole CTA: gram_smem is the per-warp Gram staging,
 // red[NP] the CTA's Gram reduction, is_last a shared flag.
-template <int B, int MODE, int FE, bool COH, bool GRAM = true>
+template <int B, int MODE, int FE, bool COH, bool GRAM = true, int L = kDefaultLpt<B>>
 __device__ __forceinline__ void pass_body(const PassParams& P, uint32_t* gram_smem, unsigned long long* red,
                                           bool& is_last) {
-  using S = Shape<B>;
+  using S = Shape<B, L>;
   constexpr int LPT = S::LPT, NV = S::NV, TPR = S::TPR, RPW = S::RPW;
   constexpr int NP = B * (B + 1) / 2;  // pairs in padded space
   constexpr bool kMma = B >= 8;
-  using Gram = typename std::conditional<kMma, GramMma<B, FE>, GramCore<B, FE>>::type;
+  using Gram = typename std::conditional<kMma, GramMma<B, FE, L>, GramCore<B, FE, L>>::type;
 
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
@@ -487,7 +490,7 @@ __device__ __forceinline__ void pass_body(const PassParams& P, uint32_t* gram_sm
             h[S::lane_of(sub, l)] = 0;
           }
         } else {
-          gather_sum<B, FE, COH>(P.cv, P.rowptr[r], P.rowptr[r + 1], 1u, P.X, sub, M, acc);
+          gather_sum<B, FE, COH, L>(P.cv, P.rowptr[r], P.rowptr[r + 1], 1u, P.X, sub, M, acc);
         }
 #pragma unroll
         for (int l = 0; l < LPT; ++l) t[l] = redc(acc[l], M);  // t = (row sum) R^{-1}
@@ -971,7 +974,7 @@ __device__ bool grid_barrier(unsigned int* bar, int* error, uint64_t limit_ns, u
 // over the stacked rows of A, grid barrier, pass over the rows of A^T, grid
 // barrier.  The blocks are read with coherent loads (they change between
 // barriers); the Gram partials go to the per-(matrix, term) slots.
-template <int B, int FE>
+template <int B, int FE, int L>
 __global__ void __launch_bounds__(kThreads, (B >= 32 ? 2 : 4)) persistent_kernel(PersistParams Q) {
   extern __shared__ __align__(16) uint32_t gram_smem[];
   __shared__ unsigned long long red[B * (B + 1) / 2];
@@ -982,13 +985,13 @@ __global__ void __launch_bounds__(kThreads, (B >= 32 ? 2 : 4)) persistent_kernel
     P.X = Q.X[cur];
     P.Y = Q.U;
     P.term = 2 * t + 1;
-    pass_body<B, kModeOdd, FE, true>(P, gram_smem, red, is_last);
+    pass_body<B, kModeOdd, FE, true, true, L>(P, gram_smem, red, is_last);
     if (!grid_barrier(Q.bar, Q.error, Q.limit_ns, gridDim.x)) return;
     P = Q.even;
     P.X = Q.U;
     P.Y = Q.X[cur ^ 1];
     P.term = 2 * t + 2;
-    pass_body<B, kModeEven, FE, true>(P, gram_smem, red, is_last);
+    pass_body<B, kModeEven, FE, true, true, L>(P, gram_smem, red, is_last);
     if (!grid_barrier(Q.bar, Q.error, Q.limit_ns, gridDim.x)) return;
     cur ^= 1;
   }
@@ -1261,47 +1264,64 @@ int launch_pass_raw(cudaStream_t s, int B, int fold4, int grid, const PassParams
   return fail(RR_EINVAL, "unsupported padded block width %d", B);
 }
 
-template <int B>
-static int launch_persistent_B(cudaStream_t s, int fold4, int grid, PersistParams& Q) {
+template <int B, int L>
+static int launch_persistent_BL(cudaStream_t s, int fold4, int grid, PersistParams& Q) {
   const size_t sm = pass_smem_bytes<B>();
   void* args[] = {&Q};
   // the shared-memory limit was raised by persistent_blocks_per_sm at set-up
-  const void* fn = fold4 ? (const void*)persistent_kernel<B, 4> : (const void*)persistent_kernel<B, 2>;
+  const void* fn = fold4 ? (const void*)persistent_kernel<B, 4, L> : (const void*)persistent_kernel<B, 2, L>;
   RR_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kThreads), args, sm, s));
   return RR_OK;
 }
 
-int launch_persistent_raw(cudaStream_t s, int B, int fold4, int grid, PersistParams& Q) {
-  switch (B) {
-    case 4: return launch_persistent_B<4>(s, fold4, grid, Q);
-    case 8: return launch_persistent_B<8>(s, fold4, grid, Q);
-    case 16: return launch_persistent_B<16>(s, fold4, grid, Q);
-    case 32: return launch_persistent_B<32>(s, fold4, grid, Q);
-  }
-  return fail(RR_EINVAL, "unsupported padded block width %d", B);
-}
-
-template <int B>
-static int persistent_blocks_B(int fold4, int* blocks) {
+template <int B, int L>
+static int persistent_blocks_BL(int fold4, int* blocks) {
   const size_t sm = pass_smem_bytes<B>();
   if (fold4) {
-    RR_CUDA(cudaFuncSetAttribute(persistent_kernel<B, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, persistent_kernel<B, 4>, kThreads, sm));
+    RR_CUDA(cudaFuncSetAttribute(persistent_kernel<B, 4, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, persistent_kernel<B, 4, L>, kThreads, sm));
   } else {
-    RR_CUDA(cudaFuncSetAttribute(persistent_kernel<B, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, persistent_kernel<B, 2>, kThreads, sm));
+    RR_CUDA(cudaFuncSetAttribute(persistent_kernel<B, 2, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, persistent_kernel<B, 2, L>, kThreads, sm));
   }
   return RR_OK;
 }
 
-int persistent_blocks_per_sm(int B, int fold4, int* blocks) {
-  switch (B) {
-    case 4: return persistent_blocks_B<4>(fold4, blocks);
-    case 8: return persistent_blocks_B<8>(fold4, blocks);
-    case 16: return persistent_blocks_B<16>(fold4, blocks);
-    case 32: return persistent_blocks_B<32>(fold4, blocks);
+// Lanes per thread the persistent kernel is built for at padded width B.
+int persistent_lane_options(int B, int* opts) {
+  if (B == 4) {
+    opts[0] = 4;
+    return 1;
   }
-  return fail(RR_EINVAL, "unsupported padded block width %d", B);
+  opts[0] = 4;
+  opts[1] = 8;
+  return 2;
+}
+
+int launch_persistent_raw(cudaStream_t s, int B, int fold4, int grid, int lpt, PersistParams& Q) {
+  switch (B * 100 + lpt) {
+    case 404: return launch_persistent_BL<4, 4>(s, fold4, grid, Q);
+    case 804: return launch_persistent_BL<8, 4>(s, fold4, grid, Q);
+    case 808: return launch_persistent_BL<8, 8>(s, fold4, grid, Q);
+    case 1604: return launch_persistent_BL<16, 4>(s, fold4, grid, Q);
+    case 1608: return launch_persistent_BL<16, 8>(s, fold4, grid, Q);
+    case 3204: return launch_persistent_BL<32, 4>(s, fold4, grid, Q);
+    case 3208: return launch_persistent_BL<32, 8>(s, fold4, grid, Q);
+  }
+  return fail(RR_EINVAL, "no persistent kernel for width %d and %d lanes per thread", B, lpt);
+}
+
+int persistent_blocks_per_sm(int B, int fold4, int lpt, int* blocks) {
+  switch (B * 100 + lpt) {
+    case 404: return persistent_blocks_BL<4, 4>(fold4, blocks);
+    case 804: return persistent_blocks_BL<8, 4>(fold4, blocks);
+    case 808: return persistent_blocks_BL<8, 8>(fold4, blocks);
+    case 1604: return persistent_blocks_BL<16, 4>(fold4, blocks);
+    case 1608: return persistent_blocks_BL<16, 8>(fold4, blocks);
+    case 3204: return persistent_blocks_BL<32, 4>(fold4, blocks);
+    case 3208: return persistent_blocks_BL<32, 8>(fold4, blocks);
+  }
+  return fail(RR_EINVAL, "no persistent kernel for width %d and %d lanes per thread", B, lpt);
 }
 
 int launch_barrier_check(cudaStream_t s, int grid, unsigned int* bar, int* error, uint64_t limit_ns,
@@ -1334,14 +1354,9 @@ int pass_blocks_per_sm(int B, int fold4, int* blocks) {
   return fail(RR_EINVAL, "unsupported padded block width %d", B);
 }
 
-int rows_per_batch(int B) {
-  switch (B) {
-    case 4: return Shape<4>::RPW;
-    case 8: return Shape<8>::RPW;
-    case 16: return Shape<16>::RPW;
-    case 32: return Shape<32>::RPW;
-  }
-  return 0;
+int rows_per_batch(int B, int lpt) {
+  if (lpt <= 0) lpt = B >= 16 ? 8 : 4;
+  return 32 * lpt / B;  // 32 / threads per row
 }
 
 int krylov_occupancy(rr_krylov* kr) {

@@ -79,9 +79,13 @@ struct PersistParams {
   int* error;
   uint64_t limit_ns;
 };
-int launch_persistent_raw(cudaStream_t s, int B, int fold4, int grid, PersistParams& Q);
+// lpt: lanes of the block per thread (4 or 8; persistent_lane_options).
+int launch_persistent_raw(cudaStream_t s, int B, int fold4, int grid, int lpt, PersistParams& Q);
 // Largest co-resident CTAs per SM of the persistent kernel (sets its shared-memory limit).
-int persistent_blocks_per_sm(int B, int fold4, int* blocks);
+int persistent_blocks_per_sm(int B, int fold4, int lpt, int* blocks);
+// The lanes-per-thread variants of the persistent kernel at padded width B
+// (into opts[2]); returns their count.
+int persistent_lane_options(int B, int* opts);
 // Cooperative launch of `grid` CTAs passing `rounds` barriers that wait for `expected` arrivals.
 int launch_barrier_check(cudaStream_t s, int grid, unsigned int* bar, int* error, uint64_t limit_ns,
                          unsigned int expected, int rounds);
@@ -95,8 +99,9 @@ int launch_batch_finalize(cudaStream_t s, const unsigned long long* gram_all, co
 int launch_pass_raw(cudaStream_t s, int B, int fold4, int grid, const PassParams& P, int mode);
 // CTAs per SM of the pass kernel for padded width B (also sets its shared-memory limit).
 int pass_blocks_per_sm(int B, int fold4, int* blocks);
-// Rows per warp batch for padded width B.
-int rows_per_batch(int B);
+// Rows per warp batch for padded width B with lpt lanes per thread (0: the
+// default shape of the pass kernels).
+int rows_per_batch(int B, int lpt = 0);
 // Warps per CTA of the pass kernel.
 constexpr int kPassWarps = 8;
 // Copies of the Gram accumulators: CTAs spread their 64-bit atomics over

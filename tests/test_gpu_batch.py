@@ -136,7 +136,8 @@ def test_batch_graph_complex_subset(ctx):
 
 def test_batch_autotuner_shapes(ctx):
     """The autotuner picks, per phase of the Krylov loop, a grid of 1..4 CTAs
-    per SM; phases start at increasing applications; results stay exact."""
+    per SM and the lanes each thread owns; phases start at increasing
+    applications; results stay exact."""
     b = 8
     mats = _mixed_batch(31, count=7)
     drs, dcs, vs = _inputs(mats, b, 13)
@@ -145,6 +146,9 @@ def test_batch_autotuner_shapes(ctx):
     assert len(shapes) >= 1 and shapes[0][0] == 0
     assert all(s1[0] > s0[0] for s0, s1 in zip(shapes, shapes[1:]))
     assert all(c % 148 == 0 and 148 <= c <= 4 * 148 for _, c in shapes) or all(c >= 1 for _, c in shapes)
+    lanes = bt.tuning_shape()  # block shape beside the grid: 4 or 8 lanes per thread at padded width 8
+    assert len(lanes) == len(shapes)
+    assert all(lpt in (4, 8) and rows == 32 * lpt // 8 for lpt, rows in lanes)
     bt.krylov()
     for i, (rowptr, col, val, m, n) in enumerate(mats):
         L = rr.default_max_nlen(m, n, b)
