@@ -260,7 +260,7 @@ def rank_pipeline(ctx, reps=3):
             "timing": "wall clock of rr_rank on a resident matrix, median of %d" % reps}
 
 
-def batched_vs_plain(ctx, nmat=48, rmin=1000, rmax=20000, b=16, workers=4):
+def batched_vs_plain(ctx, nmat=256, rmin=1000, rmax=200_000, b=16, workers=4, runs=1):
     """Graph-complex-like batch (rows log-uniform, cols = rows * U(0.6, 1), 3..10
     entries +-1 per row, planted deficits): the batched engine (rr_batch_*)
     against the plain one-matrix-at-a-time GPU loop (rr_rank) on the same set."""
@@ -283,9 +283,9 @@ def batched_vs_plain(ctx, nmat=48, rmin=1000, rmax=20000, b=16, workers=4):
         rr.block_wiedemann_rank(rr.CsrMatrix.from_arrays(*mats[i]).to_device(P, ctx), b, P, row_precond=drs[i],
                                 col_precond=dcs[i], v=vs[i], ctx=ctx)
     # the batched time varies from run to run (host threads, generator
-    # scheduling): the median of three runs is reported, with all three
+    # scheduling): the median of `runs` runs is reported, with all of them
     t_runs = []
-    for _ in range(3):
+    for _ in range(runs):
         t0 = time.perf_counter()
         bt = rr.Batch(mats, b, P, drs, dcs, vs, ctx)
         ranks = bt.ranks(workers)
@@ -300,16 +300,21 @@ def batched_vs_plain(ctx, nmat=48, rmin=1000, rmax=20000, b=16, workers=4):
         dm.close()
     t_plain = time.perf_counter() - t0
     assert list(ranks) == plain, "batched ranks differ from the plain loop"
+    shapes = []
+    bt = rr.Batch(mats[: min(nmat, 8)], b, P, drs[:8], dcs[:8], vs[:8], ctx)
+    shapes = [{"apps_from": a, "ctas": c, "lanes_per_thread": l, "rows_per_warp": r}
+              for (a, c), (l, r) in zip(bt.tuning(), bt.tuning_shape())]
+    bt.close()
     return {"workload": f"graph_complex_batch_{nmat}_rows_{rmin}-{rmax}_b{b}",
-            "note": "rows scaled from 1000-200000 to keep the run within the bench's time budget",
             "matrices": nmat, "batched_ranks_per_sec": nmat / t_batch, "plain_ranks_per_sec": nmat / t_plain,
+            "tuned_shapes_first8": shapes,
             "batched_over_plain": t_plain / t_batch, "batched_s": t_batch, "batched_runs_s": t_runs,
             "plain_s": t_plain,
             "timing": "wall clock, host matrices in, ranks out (upload, Krylov, generator, readout), after one "
-                  "untimed warm-up of both modes on a subset; batched: median of 3 runs"}
+                  "untimed warm-up of both modes on a subset; batched: median of %d run(s)" % runs}
 
 
-def served_stream(nreq=40, rmin=10_000, rmax=100_000, rate=50.0, b=16, seed=48):
+def served_stream(nreq=12, rmin=10_000, rmax=2_000_000, rate=50.0, b=16, seed=48):
     """Poisson arrivals (mean `rate` req/s) of rank requests (rows log-uniform,
     4..12 entries +-1 per row) through the rank service (rr_server_*), against
     the plain sequential GPU loop on the same requests."""
@@ -361,12 +366,35 @@ def served_stream(nreq=40, rmin=10_000, rmax=100_000, rate=50.0, b=16, seed=48):
     ctx.close()
     assert served == plain, "served ranks differ from the plain loop"
     return {"workload": f"served_poisson_{rate:g}rps_{nreq}req_rows_{rmin}-{rmax}_nnz4-12_b{b}",
-            "note": "rows scaled from 10^4-2*10^6 to keep the run within the bench's time budget",
             "requests": nreq, "served_ranks_per_sec": st["ranks_per_s"], "p50_ms": st["p50_ms"],
             "p99_ms": st["p99_ms"], "plain_ranks_per_sec": nreq / t_plain,
             "served_over_plain": st["ranks_per_s"] / (nreq / t_plain),
             "timing": "latency = submit to rank (queueing included); throughput = completions / (last completion - "
                       "first submit); plain = sequential upload + rr_rank per request; one untimed warm-up service run"}
+
+
+def full_rank_zipf(ctx, rowptr, col, val, m, n, b=16):
+    """Host CSR in, rank out on the large Zipf matrix: rr_matrix_create (device
+    build), the Krylov sequence of the stated length N/b + N/b + 32 (N = the
+    smaller dimension), the PM-basis of order d = largest power of two <= length,
+    and the rank readout -- all through the public API, timed by wall clock."""
+    import rust_rank_b200 as rr
+    from rust_rank_b200 import synth
+
+    dr, dc = synth.preconditioners(m, n, P, 61)
+    V = synth.random_vectors(b, n, P, 62)
+    L = 2 * (min(m, n) // b) + 32
+    t0 = time.perf_counter()
+    dm = rr.CsrMatrix.from_arrays(rowptr, col, val, m, n).to_device(P, ctx)
+    t1 = time.perf_counter()
+    rank = rr.block_wiedemann_rank(dm, b, P, row_precond=dr, col_precond=dc, v=V, max_nlen=L, ctx=ctx)
+    t2 = time.perf_counter()
+    dm.close()
+    nonempty = int(np.count_nonzero(np.bincount(col, minlength=n)))
+    return {"workload": f"zipf_{m}x{n}_nnz{int(rowptr[-1])}_b{b}", "sequence_terms": L + 1, "rank": rank,
+            "upper_bound_nonempty_columns": nonempty, "s_total": t2 - t0, "s_matrix_build": t1 - t0,
+            "ranks_per_sec": 1.0 / (t2 - t0),
+            "timing": "wall clock, host CSR in (pageable numpy arrays), rank out"}
 
 
 def pm_basis_stage(ctx, b=16, ds=(1 << 14, 1 << 16)):
@@ -501,9 +529,10 @@ def run_engine(args):
     # otherwise share the host cores with the engine's host threads
     if rank == 0 and world == 1 and not args.no_rank:
         line["rank_pipeline"] = rank_pipeline(ctx)
+        line["pm_basis"] = pm_basis_stage(ctx)
+        line["full_rank"] = full_rank_zipf(ctx, rowptr, col, val, m, n, b)
         line["batched"] = batched_vs_plain(ctx)
         line["served"] = served_stream()
-        line["pm_basis"] = pm_basis_stage(ctx)
     if rank == 0 and world == 1 and args.cpu_samples > 0:
         v, dt, threads = cpu_baseline(rowptr, col, val, m, n, b, args.cpu_samples)
         line["cpu_baseline"] = {"value": v, "unit": "GB/s", "cores": threads, "kind": "port",
