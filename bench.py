@@ -405,14 +405,29 @@ def pm_basis_stage(ctx, b=16, ds=(1 << 14, 1 << 16)):
     rng = np.random.default_rng(4)
     for d in ds:
         seq = rng.integers(0, P, size=(b * (b + 1) // 2, d + 1), dtype=np.int64).astype(np.uint32)
+        for tc in (True, False):
+            ctx.set_pm_tensor_cores(tc)
+            best, ref = None, None
+            for _ in range(2):  # the first call also grows the memory pool to this size's workspace
+                t0 = time.perf_counter()
+                M, delta = rr.PM_Basis(seq, d, P, ctx)
+                dt = time.perf_counter() - t0
+                best = dt if best is None else min(best, dt)
+            out[f"d{d}_ms" if tc else f"d{d}_cuda_core_ms"] = 1e3 * best
+        ctx.set_pm_tensor_cores(True)
+    for p_small in (3323,):  # a prime without a suitable NTT: products by CRT over NTT primes
+        d = ds[0]
+        seq = rng.integers(0, p_small, size=(b * (b + 1) // 2, d + 1), dtype=np.int64).astype(np.uint32)
         best = None
-        for _ in range(2):  # the first call also grows the memory pool to this size's workspace
+        for _ in range(2):
             t0 = time.perf_counter()
-            rr.PM_Basis(seq, d, P, ctx)
+            rr.PM_Basis(seq, d, p_small, ctx)
             dt = time.perf_counter() - t0
             best = dt if best is None else min(best, dt)
-        out[f"d{d}_ms"] = 1e3 * best
+        out[f"d{d}_p{p_small}_ms"] = 1e3 * best
     out["workload"] = f"pm_basis_b{b}_2b{2 * b}_uniform_random_seq"
+    out["contractions"] = ("dN_ms: leaf residual updates and block-basis products on the int8 tensor cores "
+                           "(byte limbs, exact); dN_cuda_core_ms: the same on the CUDA cores (64-bit sums)")
     out["timing"] = "wall clock of rr_pm_basis (host sequence in, generator out), best of 2"
     return out
 

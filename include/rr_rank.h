@@ -52,6 +52,12 @@ int rr_ctx_destroy(rr_ctx* ctx);
 /* The cudaStream_t (as void*) all work of this context is queued on. */
 void* rr_ctx_stream(rr_ctx* ctx);
 int rr_ctx_synchronize(rr_ctx* ctx);
+/* PM-basis contractions of this context (the leaf residual updates and the
+ * block-basis products): on the int8 tensor cores by byte limbs (enable = 1,
+ * the default, for b <= 16) or on the CUDA cores with 64-bit sums (0).  The
+ * generator is the same bit for bit; this selects the path, e.g. to compare
+ * them.  No counterpart in the reference. */
+int rr_ctx_set_pm_tensor_cores(rr_ctx* ctx, int32_t enable);
 
 /* ---------------------------------------------------------------- checks */
 /* RR_OK when p is a prime with 2 < p < 2^31, the range the engine computes

@@ -69,6 +69,10 @@ class Context:
     def stream(self) -> int:
         return lib().rr_ctx_stream(self.handle) or 0
 
+    def set_pm_tensor_cores(self, enable: bool):
+        """PM-basis contractions on the int8 tensor cores (True, default) or the CUDA cores (False)."""
+        check(lib().rr_ctx_set_pm_tensor_cores(self.handle, 1 if enable else 0))
+
     def synchronize(self):
         check(lib().rr_ctx_synchronize(self.handle))
 

@@ -31,6 +31,7 @@ SIGNATURES = {
     "rr_ctx_destroy": (C.c_int, [_vp]),
     "rr_ctx_stream": (_vp, [_vp]),
     "rr_ctx_synchronize": (C.c_int, [_vp]),
+    "rr_ctx_set_pm_tensor_cores": (C.c_int, [_vp, _i32]),
     "rr_prime_check": (C.c_int, [_u32]),
     "rr_matrix_create": (C.c_int, [_vp, _i64, _i64, _vp, _vp, _vp, _u32, C.POINTER(_vp)]),
     "rr_matrix_destroy": (C.c_int, [_vp]),

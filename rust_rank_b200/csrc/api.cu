@@ -204,6 +204,12 @@ int rr_ctx_destroy(rr_ctx* ctx) {
 
 void* rr_ctx_stream(rr_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
+int rr_ctx_set_pm_tensor_cores(rr_ctx* ctx, int32_t enable) {
+  if (!ctx) return fail(RR_EINVAL, "NULL context");
+  ctx->pm_tensor_cores = enable ? 1 : 0;
+  return RR_OK;
+}
+
 int rr_ctx_synchronize(rr_ctx* ctx) {
   if (!ctx) return fail(RR_EINVAL, "ctx is NULL");
   RR_CUDA(cudaSetDevice(ctx->device));

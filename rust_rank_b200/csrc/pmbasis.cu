@@ -1793,7 +1793,7 @@ int pm_basis_batch_device(rr_ctx* ctx, int nb, const uint32_t* const* seqs, cons
   P.p = p;
   P.M = make_modp(p);
   size_t leaves_smem = 0;
-  P.mma = P.m <= kMmaRows && P.n <= kMmaCols;
+  P.mma = ctx->pm_tensor_cores && P.m <= kMmaRows && P.n <= kMmaCols;
   P.K = pick_block_leaves(P.m, P.n, d, P.mma, &leaves_smem);
   P.cs = leaf_coeff_stride(P.m, P.n);
   P.fold4 = fold4_ok(p, P.M);

@@ -127,6 +127,7 @@ struct rr_ctx_s {
   int device = 0;
   cudaStream_t stream = nullptr;
   int num_sms = 0;
+  int pm_tensor_cores = 1;  // PM-basis contractions on the int8 tensor cores (0: CUDA cores)
 };
 
 namespace rr {

@@ -94,3 +94,21 @@ def test_batched_pm_basis_small_prime_golden(ctx, golden):
         got = rr.PM_Basis_batch([z[f"c{i}_seq"] for i in idx], d, 3323, ctx)
         for i, (M, delta) in zip(idx, got):
             assert np.array_equal(M, z[f"c{i}_M"]) and np.array_equal(delta, z[f"c{i}_delta"]), i
+
+
+@pytest.mark.parametrize("b,d", [(8, 256), (16, 512), (16, 33), (4, 64)])
+def test_cuda_core_contractions_equal_tensor_core(b, d):
+    """The leaf residual updates and block-basis products on the CUDA cores
+    (rr_ctx_set_pm_tensor_cores(ctx, 0)) give the tensor-core generator and the
+    oracle's, bit for bit."""
+    c = rr.Context(0)
+    rng = np.random.default_rng(b * 7 + d)
+    dd = 1 << (d - 1).bit_length()
+    seq = rng.integers(0, P, size=(b * (b + 1) // 2, dd + 2)).astype(np.uint32)
+    M_tc, d_tc = rr.PM_Basis(seq, d, P, c)
+    c.set_pm_tensor_cores(False)
+    M_cc, d_cc = rr.PM_Basis(seq, d, P, c)
+    c.close()
+    Mo, do = oracle.pm_basis(seq, b, d, P)
+    assert np.array_equal(M_cc, M_tc) and np.array_equal(d_cc, d_tc)
+    assert np.array_equal(M_cc, Mo.astype(np.uint32)) and np.array_equal(d_cc, do)
