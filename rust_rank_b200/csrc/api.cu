@@ -102,37 +102,6 @@ int krylov_reserve(rr_krylov* kr, int64_t terms) {
   RR_CUDA(cudaSetDevice(kr->mat->ctx->device));
   return ensure_capacity(kr, terms);
 }
-// The L2 set-aside for persisting accesses (a limit of this process's
-// context, raised once per device to the device's maximum) and the window
-// marking U persisting: U is written by the pass over A and gathered at random
-// rows by the pass over A^T, and it is larger than what L2 keeps by default.
-namespace {
-std::mutex g_l2_mutex;
-bool g_l2_set[64] = {};
-}  // namespace
-
-int krylov_l2_policy(rr_krylov* kr) {
-  const int dev = kr->mat->ctx->device;
-  int maxwin = 0, maxpers = 0;
-  RR_CUDA(cudaDeviceGetAttribute(&maxwin, cudaDevAttrMaxAccessPolicyWindowSize, dev));
-  RR_CUDA(cudaDeviceGetAttribute(&maxpers, cudaDevAttrMaxPersistingL2CacheSize, dev));
-  if (maxwin <= 0 || maxpers <= 0 || !kr->U.ptr || dev < 0 || dev >= 64) return RR_OK;
-  {
-    std::lock_guard<std::mutex> lk(g_l2_mutex);
-    if (!g_l2_set[dev]) {
-      RR_CUDA(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, (size_t)maxpers));
-      g_l2_set[dev] = true;
-    }
-  }
-  const size_t bytes = std::min(kr->U.bytes(), (size_t)maxwin);
-  kr->l2win.base_ptr = kr->U.ptr;
-  kr->l2win.num_bytes = bytes;
-  kr->l2win.hitRatio = (float)std::min(1.0, (double)maxpers / (double)bytes);
-  kr->l2win.hitProp = cudaAccessPropertyPersisting;
-  kr->l2win.missProp = cudaAccessPropertyStreaming;
-  return RR_OK;
-}
-
 }  // namespace rr
 
 extern "C" {
@@ -333,7 +302,6 @@ int rr_krylov_create(rr_matrix* mat, int32_t b, const uint32_t* row_precond, con
     RR_CUDA(cudaStreamSynchronize(s));
   }
   RR_TRY(krylov_occupancy(kr.get()));
-  RR_TRY(krylov_l2_policy(kr.get()));
   kr->base = seq_len;
   kr->len = seq_len;
   RR_TRY(ensure_capacity(kr.get(), 64));

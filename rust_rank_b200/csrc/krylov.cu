@@ -649,7 +649,7 @@ __global__ void __launch_bounds__(kThreads, (B >= 32 && GRAM ? 2 : 4)) pass_kern
 // (tcgen05.ld), weight limb pairs by 2^{8(a+c)} mod p, and the CTA's sums join
 // the same replicated 64-bit accumulators and last-CTA finish as the pass
 // kernels.  Every wait on an mbarrier gives up after 2 s and sets *status.
-constexpr int kTcRows = 128;        // rows (K bytes) per tile
+constexpr int kTcRows = 256;        // rows (K bytes) per tile
 constexpr int kTcDrain = 64;        // tiles between drains of the int32 accumulators
 constexpr uint64_t kTcWaitLimitNs = 2000000000ull;  // 2 s of %globaltimer
 
@@ -705,8 +705,43 @@ constexpr size_t gram_tc_smem_bytes() {
   return 2 * (size_t)(TcShape<B>::A_BYTES + TcShape<B>::B_BYTES);
 }
 
+// One staging task: 4 consecutive rows x 4 lanes (one 128-bit word per row)
+// of the block and the 4 row scales, loaded a tile ahead.
 template <int B>
-__global__ void __launch_bounds__(kThreads, 2) gram_tc_kernel(PassParams P, int* status) {
+struct TcLoad {
+  static constexpr int GROUPS = B / 4;                    // 128-bit words per row
+  static constexpr int TASKS = (kTcRows / 4) * GROUPS;    // per tile
+  static constexpr int TPT = TASKS / kThreads;            // per thread
+  uint4 y[TPT][4];
+  uint32_t sc[TPT][4];
+  __device__ __forceinline__ void load(const PassParams& P, int64_t tile, int tid) {
+#pragma unroll
+    for (int t = 0; t < TPT; ++t) {
+      const int task = tid + t * kThreads, g = task % GROUPS, qd = task / GROUPS;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int64_t r = tile * kTcRows + 4 * qd + q;
+        const bool in = r < P.rows;
+        y[t][q] = in ? __ldg(P.X + r * GROUPS + g) : make_uint4(0, 0, 0, 0);
+        sc[t][q] = in ? __ldg(P.scale + r) : 0u;
+      }
+    }
+  }
+};
+static_assert(TcLoad<16>::TASKS % kThreads == 0 && TcLoad<32>::TASKS % kThreads == 0, "staging tasks");
+
+__device__ __forceinline__ void byte_transpose4(const uint32_t (&v)[4], uint32_t (&w)[4]) {
+  // w[a] = bytes a of v[0..3]: limb a of four consecutive rows
+  const uint32_t t0 = __byte_perm(v[0], v[1], 0x5140), t1 = __byte_perm(v[2], v[3], 0x5140);
+  const uint32_t t2 = __byte_perm(v[0], v[1], 0x7362), t3 = __byte_perm(v[2], v[3], 0x7362);
+  w[0] = __byte_perm(t0, t1, 0x5410);
+  w[1] = __byte_perm(t0, t1, 0x7632);
+  w[2] = __byte_perm(t2, t3, 0x5410);
+  w[3] = __byte_perm(t2, t3, 0x7632);
+}
+
+template <int B>
+__global__ void __launch_bounds__(kThreads, (B >= 32 ? 1 : 2)) gram_tc_kernel(PassParams P, int* status) {
   using T = TcShape<B>;
   constexpr int NP = B * (B + 1) / 2;
   extern __shared__ __align__(1024) unsigned char tc_smem[];
@@ -796,6 +831,8 @@ __global__ void __launch_bounds__(kThreads, 2) gram_tc_kernel(PassParams P, int*
   const int64_t ntiles = (P.rows + kTcRows - 1) / kTcRows;
   int64_t tl = 0;        // tiles of this CTA so far
   bool acc_live = false;  // D holds sums to accumulate onto
+  TcLoad<B> cur;
+  if ((int64_t)blockIdx.x < ntiles) cur.load(P, blockIdx.x, tid);
   for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++tl) {
     const int s = (int)(tl & 1);
     unsigned char* const bufA = tc_smem + s * (T::A_BYTES + T::B_BYTES);
@@ -808,52 +845,41 @@ __global__ void __launch_bounds__(kThreads, 2) gram_tc_kernel(PassParams P, int*
       __syncthreads();
     }
     if (s_fail) break;
-    // stage: 32 row-quads x B lanes; 4 rows of one lane become one word per limb
-    const int64_t r0 = tile * kTcRows;
-    for (int task = tid; task < 32 * B; task += kThreads) {
-      const int i = task % B, qd = task / B;
-      uint32_t z[4], u[4];
+    // stage the tile loaded a round ago, with the next tile's loads already in flight
+    TcLoad<B> nxt;
+    if (tile + gridDim.x < ntiles) nxt.load(P, tile + gridDim.x, tid);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int64_t r = r0 + 4 * qd + q;
-        uint32_t y = 0, sc = 0;
-        if (r < P.rows) {
-          y = __ldg(reinterpret_cast<const uint32_t*>(P.X) + r * B + i);
-          sc = __ldg(P.scale + r);
+    for (int t = 0; t < TcLoad<B>::TPT; ++t) {
+      const int task = tid + t * kThreads, g = task % TcLoad<B>::GROUPS, qd = task / TcLoad<B>::GROUPS;
+#pragma unroll
+      for (int c4 = 0; c4 < 4; ++c4) {
+        const int i = 4 * g + c4;
+        uint32_t z[4], u[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const uint4 y4 = cur.y[t][q];
+          const uint32_t y = c4 == 0 ? y4.x : c4 == 1 ? y4.y : c4 == 2 ? y4.z : y4.w;
+          z[q] = redc((uint64_t)y * cur.sc[t][q], M);
+          u[q] = P.gram_sym ? z[q] : y;
         }
-        z[q] = redc((uint64_t)y * sc, M);
-        u[q] = P.gram_sym ? z[q] : y;
-      }
-      uint32_t wz[4], wu[4];
-      {
-        const uint32_t t0 = __byte_perm(z[0], z[1], 0x5140), t1 = __byte_perm(z[2], z[3], 0x5140);
-        const uint32_t t2 = __byte_perm(z[0], z[1], 0x7362), t3 = __byte_perm(z[2], z[3], 0x7362);
-        wz[0] = __byte_perm(t0, t1, 0x5410);
-        wz[1] = __byte_perm(t0, t1, 0x7632);
-        wz[2] = __byte_perm(t2, t3, 0x5410);
-        wz[3] = __byte_perm(t2, t3, 0x7632);
-      }
-      {
-        const uint32_t t0 = __byte_perm(u[0], u[1], 0x5140), t1 = __byte_perm(u[2], u[3], 0x5140);
-        const uint32_t t2 = __byte_perm(u[0], u[1], 0x7362), t3 = __byte_perm(u[2], u[3], 0x7362);
-        wu[0] = __byte_perm(t0, t1, 0x5410);
-        wu[1] = __byte_perm(t0, t1, 0x7632);
-        wu[2] = __byte_perm(t2, t3, 0x5410);
-        wu[3] = __byte_perm(t2, t3, 0x7632);
-      }
+        uint32_t wz[4], wu[4];
+        byte_transpose4(z, wz);
+        byte_transpose4(u, wu);
 #pragma unroll
-      for (int a = 0; a < 4; ++a) {
-        *reinterpret_cast<uint32_t*>(bufA + tc_off(T::M, a * B + i, 4 * qd)) = wz[a];
-        *reinterpret_cast<uint32_t*>(bufB + tc_off(T::N, a * B + i, 4 * qd)) = wu[a];
+        for (int a = 0; a < 4; ++a) {
+          *reinterpret_cast<uint32_t*>(bufA + tc_off(T::M, a * B + i, 4 * qd)) = wz[a];
+          *reinterpret_cast<uint32_t*>(bufB + tc_off(T::N, a * B + i, 4 * qd)) = wu[a];
+        }
       }
     }
+    cur = nxt;
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint32_t a0 = smem_u32(bufA), b0 = smem_u32(bufB);
 #pragma unroll
-      for (int kb = 0; kb < 4; ++kb) {
+      for (int kb = 0; kb < kTcRows / 32; ++kb) {
         const uint64_t da = umma_desc(a0 + kb * (T::M / 8) * 256);
         const uint64_t db = umma_desc(b0 + kb * (T::N / 8) * 256);
         const uint32_t accum = (acc_live || kb > 0) ? 1u : 0u;
@@ -1121,23 +1147,16 @@ static int pass_grid_lean(const rr_krylov* kr, int64_t rows) {
   return (int)std::max<int64_t>(1, std::min<int64_t>(kr->grid_lean, need));
 }
 
-// A launch with the handle's L2 access policy window (U persisting) as a
-// per-launch attribute: no stream state changes, and captured launches keep it.
+// Kernel launches of the single-matrix path, through cudaLaunchKernelEx.
 template <class... Args>
-static int launch_with_l2(const rr_krylov* kr, void (*fn)(Args...), dim3 grid, dim3 block, size_t smem,
+static int launch_ex(const rr_krylov* kr, void (*fn)(Args...), dim3 grid, dim3 block, size_t smem,
                           cudaStream_t s, Args... args) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
   cfg.blockDim = block;
   cfg.dynamicSmemBytes = smem;
   cfg.stream = s;
-  cudaLaunchAttribute attr[1];
-  if (kr->l2win.num_bytes > 0) {
-    attr[0].id = cudaLaunchAttributeAccessPolicyWindow;
-    attr[0].val.accessPolicyWindow = kr->l2win;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-  }
+  (void)kr;
   RR_CUDA(cudaLaunchKernelEx(&cfg, fn, args...));
   return RR_OK;
 }
@@ -1151,10 +1170,10 @@ static int launch_pass_BF(rr_krylov* kr, const PassParams& P, int mode, dim3 gri
   const dim3 block(kThreads);
   const size_t sm = pass_smem_bytes<B>();
   switch (mode) {
-    case kModeInit: return launch_with_l2(kr, pass_kernel<B, kModeInit, FE, true>, grid, block, sm, s, P);
-    case kModeOdd: return launch_with_l2(kr, pass_kernel<B, kModeOdd, FE, false>, grid, block, 0, s, P);
-    case kModeEven: return launch_with_l2(kr, pass_kernel<B, kModeEven, FE, false>, grid, block, 0, s, P);
-    default: return launch_with_l2(kr, pass_kernel<B, kModeGram, FE, true>, grid, block, sm, s, P);
+    case kModeInit: return launch_ex(kr, pass_kernel<B, kModeInit, FE, true>, grid, block, sm, s, P);
+    case kModeOdd: return launch_ex(kr, pass_kernel<B, kModeOdd, FE, false>, grid, block, 0, s, P);
+    case kModeEven: return launch_ex(kr, pass_kernel<B, kModeEven, FE, false>, grid, block, 0, s, P);
+    default: return launch_ex(kr, pass_kernel<B, kModeGram, FE, true>, grid, block, sm, s, P);
   }
 }
 
@@ -1162,8 +1181,9 @@ static int launch_pass_BF(rr_krylov* kr, const PassParams& P, int mode, dim3 gri
 template <int B>
 static int launch_gram_tc(rr_krylov* kr, const PassParams& P, cudaStream_t s) {
   const int64_t ntiles = (P.rows + kTcRows - 1) / kTcRows;
-  const dim3 grid((unsigned)std::max<int64_t>(1, std::min<int64_t>(ntiles, 2 * (int64_t)kr->mat->ctx->num_sms)));
-  return launch_with_l2(kr, gram_tc_kernel<B>, grid, dim3(kThreads), gram_tc_smem_bytes<B>(), s, P,
+  const int per_sm = B >= 32 ? 1 : 2;
+  const dim3 grid((unsigned)std::max<int64_t>(1, std::min<int64_t>(ntiles, per_sm * (int64_t)kr->mat->ctx->num_sms)));
+  return launch_ex(kr, gram_tc_kernel<B>, grid, dim3(kThreads), gram_tc_smem_bytes<B>(), s, P,
                         kr->d_status.ptr);
 }
 
@@ -1205,8 +1225,8 @@ static int launch_chunk_B(rr_krylov* kr, const ChunkParams& P) {
   const dim3 grid((unsigned)std::max<int64_t>(1, std::min<int64_t>(kr->grid_chunk, (P.nchunks + kWarps - 1) / kWarps))),
       block(kThreads);
   cudaStream_t s = kr->launch_stream ? kr->launch_stream : kr->mat->ctx->stream;
-  if (kr->fold4) return launch_with_l2(kr, chunk_kernel<B, 4>, grid, block, 0, s, P);
-  return launch_with_l2(kr, chunk_kernel<B, 2>, grid, block, 0, s, P);
+  if (kr->fold4) return launch_ex(kr, chunk_kernel<B, 4>, grid, block, 0, s, P);
+  return launch_ex(kr, chunk_kernel<B, 2>, grid, block, 0, s, P);
 }
 
 static int launch_chunk(rr_krylov* kr, const ChunkParams& P) {

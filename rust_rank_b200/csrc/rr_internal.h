@@ -190,9 +190,6 @@ struct rr_krylov_s {
   cudaStream_t launch_stream = nullptr;  // set while capturing (a private stream), else the context's
   int graph_cur = 0;
   int64_t graph_launches = 0;
-  // U (written by the pass over A, gathered by the pass over A^T) is marked
-  // persisting in L2 for the pass launches (num_bytes == 0: not available)
-  cudaAccessPolicyWindow l2win{};
   ~rr_krylov_s() {
     if (graph) cudaGraphExecDestroy(graph);
   }
@@ -204,8 +201,6 @@ int krylov_reserve(rr_krylov* kr, int64_t terms);
 int krylov_launch_application(rr_krylov* kr, cudaEvent_t* ev);
 int krylov_launch_get_curv(rr_krylov* kr, uint32_t* d_out);
 int krylov_occupancy(rr_krylov* kr);
-// Marks the handle's U persisting in L2 for its pass launches (api.cu).
-int krylov_l2_policy(rr_krylov* kr);
 // Sequence length rule of src/main.rs:497-504; padded block width; device
 // bytes a matrix and its Krylov state hold while resident (server.cpp).
 int64_t max_nlen_for(int64_t m, int64_t n, int b);
