@@ -622,13 +622,19 @@ __device__ __forceinline__ void pass_body(const PassParams& P, uint32_t* gram_sm
 // worth a few spilled registers (measured on the 2M x 1.5M Zipf matrix).  At
 // B = 32 the Gram accumulators alone take 48 registers, and two CTAs per SM
 // with 128 registers run the same matrix 1.2x faster than four with spills.
-template <int B, int MODE, int FE, bool GRAM = true>
+template <int B, int MODE, int FE, bool GRAM = true, int L = kDefaultLpt<B>>
 __global__ void __launch_bounds__(kThreads, (B >= 32 && GRAM ? 2 : 4)) pass_kernel(PassParams P) {
   extern __shared__ __align__(16) uint32_t gram_smem[];
   __shared__ unsigned long long red[B * (B + 1) / 2];
   __shared__ bool is_last;
-  pass_body<B, MODE, FE, false, GRAM>(P, gram_smem, red, is_last);
+  pass_body<B, MODE, FE, false, GRAM, L>(P, gram_smem, red, is_last);
 }
+
+// Lanes per thread of the single-matrix odd and even passes: 4 (a whole
+// 16-lane row in one warp load instruction, one L1 line look-up per gathered
+// row) at padded width 16, the pass kernels' default otherwise.
+template <int B>
+constexpr int kLeanLpt = (B == 16) ? 4 : kDefaultLpt<B>;
 
 // ---------------------------------------------------------------- Gram pass on tcgen05
 // The Gram term of a block (kModeGram: gz = x * scale, gu = gram_sym ? gz : x
@@ -1142,7 +1148,8 @@ static int pass_grid(const rr_krylov* kr, int64_t rows) {
 
 template <int B>
 static int pass_grid_lean(const rr_krylov* kr, int64_t rows) {
-  const int64_t nbatch = (rows + Shape<B>::RPW - 1) / Shape<B>::RPW;
+  constexpr int RPW = Shape<B, kLeanLpt<B>>::RPW;
+  const int64_t nbatch = (rows + RPW - 1) / RPW;
   const int64_t need = (nbatch + kWarps - 1) / kWarps;
   return (int)std::max<int64_t>(1, std::min<int64_t>(kr->grid_lean, need));
 }
@@ -1171,8 +1178,8 @@ static int launch_pass_BF(rr_krylov* kr, const PassParams& P, int mode, dim3 gri
   const size_t sm = pass_smem_bytes<B>();
   switch (mode) {
     case kModeInit: return launch_ex(kr, pass_kernel<B, kModeInit, FE, true>, grid, block, sm, s, P);
-    case kModeOdd: return launch_ex(kr, pass_kernel<B, kModeOdd, FE, false>, grid, block, 0, s, P);
-    case kModeEven: return launch_ex(kr, pass_kernel<B, kModeEven, FE, false>, grid, block, 0, s, P);
+    case kModeOdd: return launch_ex(kr, pass_kernel<B, kModeOdd, FE, false, kLeanLpt<B>>, grid, block, 0, s, P);
+    case kModeEven: return launch_ex(kr, pass_kernel<B, kModeEven, FE, false, kLeanLpt<B>>, grid, block, 0, s, P);
     default: return launch_ex(kr, pass_kernel<B, kModeGram, FE, true>, grid, block, sm, s, P);
   }
 }
@@ -1247,12 +1254,14 @@ static int occupancy_B(rr_krylov* kr, int* pass_blocks, int* chunk_blocks, int* 
     RR_TRY((set_pass_smem<B, 4>()));
     RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(pass_blocks, pass_kernel<B, kModeGram, 4>, kThreads, sm));
     RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(chunk_blocks, chunk_kernel<B, 4>, kThreads, 0));
-    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(lean_blocks, pass_kernel<B, kModeOdd, 4, false>, kThreads, 0));
+    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(lean_blocks, pass_kernel<B, kModeOdd, 4, false, kLeanLpt<B>>,
+                                                          kThreads, 0));
   } else {
     RR_TRY((set_pass_smem<B, 2>()));
     RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(pass_blocks, pass_kernel<B, kModeGram, 2>, kThreads, sm));
     RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(chunk_blocks, chunk_kernel<B, 2>, kThreads, 0));
-    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(lean_blocks, pass_kernel<B, kModeOdd, 2, false>, kThreads, 0));
+    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(lean_blocks, pass_kernel<B, kModeOdd, 2, false, kLeanLpt<B>>,
+                                                          kThreads, 0));
   }
   return RR_OK;
 }
