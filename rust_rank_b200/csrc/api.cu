@@ -274,8 +274,9 @@ int rr_krylov_create(rr_matrix* mat, int32_t b, const uint32_t* row_precond, con
     RR_TRY(kr->dc_m.alloc_async(n, s));
     RR_TRY(kr->dc_r.alloc_async(n, s));
     RR_TRY(kr->dcinv.alloc_async(n, s));
-    RR_TRY(kr->drinv_r.alloc_async(m, s));
-    RR_TRY(kr->dcinv_r.alloc_async(n, s));
+    // + 4: the Gram pass copies row scales in 16-byte pieces
+    RR_TRY(kr->drinv_r.alloc_async(m + 4, s));
+    RR_TRY(kr->dcinv_r.alloc_async(n + 4, s));
     RR_CUDA(cudaMemcpyAsync(rp.ptr, row_precond, m * 4, cudaMemcpyHostToDevice, s));
     RR_CUDA(cudaMemcpyAsync(cp.ptr, col_precond, n * 4, cudaMemcpyHostToDevice, s));
     RR_TRY(launch_precond(kr.get(), rp.ptr, cp.ptr, mat->d_rowperm.ptr));

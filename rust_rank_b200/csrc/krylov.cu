@@ -630,11 +630,122 @@ __global__ void __launch_bounds__(kThreads, (B >= 32 && GRAM ? 2 : 4)) pass_kern
   pass_body<B, MODE, FE, false, GRAM, L>(P, gram_smem, red, is_last);
 }
 
+// ---------------------------------------------------------------- staged single-matrix passes
+// The odd and even passes of the single-matrix path without Gram terms, with
+// each warp batch's CSR entries staged in shared memory first: the batch's
+// rows are consecutive, so their entries are one contiguous run that the warp
+// copies with coalesced loads (32 entries per instruction), and every thread
+// then reads its row's entries from shared memory.  Loading the entries
+// straight from global memory costs one L1 look-up per entry per row (the
+// rows of a warp batch lie in different lines); staged, a batch's entries
+// cost a handful of look-ups, and the L1 pipe is left to the gathers.  Rows
+// longer than kHeavyDegree take their sums from heavy_acc (chunk kernel), so
+// a batch stages at most RPW * kHeavyDegree entries.
+template <int B, int FE, int L>
+__device__ __forceinline__ void gather_sum_staged(const uint2* st, uint32_t beg, uint32_t end,
+                                                  const uint4* __restrict__ X, int sub, const ModP& M,
+                                                  uint64_t (&acc)[Shape<B, L>::LPT]) {
+  constexpr int NV = Shape<B, L>::NV, TPR = Shape<B, L>::TPR;
+  constexpr int RW = B / 4;
+  const uint4* Xs = X + sub;
+  uint32_t k = beg;
+  for (; k + 3 < end; k += 4) {
+    uint2 e[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) e[u] = st[k + u];
+    uint4 g[4][NV];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) g[u][v] = __ldg(Xs + (size_t)e[u].x * RW + v * TPR);
+    mac_step<B, FE, L>(e, g, M, acc);
+  }
+  if (k < end) {
+    uint2 e[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      e[u] = st[k + u < end ? k + u : k];
+      if (k + u >= end) e[u].y = 0u;
+    }
+    uint4 g[4][NV];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) g[u][v] = __ldg(Xs + (size_t)e[u].x * RW + v * TPR);
+    mac_step<B, FE, L>(e, g, M, acc);
+  }
+}
+
+template <int B, int L, int MODE, int FE>
+__global__ void __launch_bounds__(kThreads, 4) staged_pass_kernel(PassParams P) {
+  using S = Shape<B, L>;
+  constexpr int LPT = S::LPT, NV = S::NV, TPR = S::TPR, RPW = S::RPW;
+  constexpr int CAP = RPW * (int)kHeavyDegree;
+  static_assert(RPW < 32, "row offsets of a batch are held one per lane");
+  __shared__ uint2 stage_all[kWarps][CAP];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int sub = lane % TPR, slot = lane / TPR;
+  uint2* const st = stage_all[warp];
+  const ModP M = P.M;
+  const int64_t nbatch = (P.rows + RPW - 1) / RPW;
+  const int64_t nw = (int64_t)gridDim.x * kWarps;
+  for (int64_t batch = (int64_t)blockIdx.x * kWarps + warp; batch < nbatch; batch += nw) {
+    const int64_t r0 = batch * RPW;
+    const int64_t rlast = r0 + RPW < P.rows ? r0 + RPW : P.rows;
+    uint32_t off = 0;  // lane j <= RPW: rowptr[r0 + j] (clamped to the last row)
+    if (lane <= RPW) off = P.rowptr[r0 + lane < rlast ? r0 + lane : rlast];
+    const int64_t rs = r0 > P.heavy_rows ? r0 : (P.heavy_rows < rlast ? P.heavy_rows : rlast);
+    const uint32_t beg = __shfl_sync(0xffffffffu, off, (int)(rs - r0));
+    const uint32_t end = __shfl_sync(0xffffffffu, off, (int)(rlast - r0));
+    const uint32_t my_a = __shfl_sync(0xffffffffu, off, slot);
+    const uint32_t my_e = __shfl_sync(0xffffffffu, off, slot + 1);
+    __syncwarp();  // the previous batch has finished reading st
+    for (uint32_t k = lane; k < end - beg; k += 32) st[k] = __ldg(P.cv + beg + k);
+    __syncwarp();
+    const int64_t r = r0 + slot;
+    if (r >= P.rows) continue;
+    uint64_t acc[LPT];
+#pragma unroll
+    for (int l = 0; l < LPT; ++l) acc[l] = 0;
+    if (r < P.heavy_rows) {
+      unsigned long long* h = P.heavy_acc + (size_t)r * B;
+#pragma unroll
+      for (int l = 0; l < LPT; ++l) {
+        acc[l] = fold(h[S::lane_of(sub, l)], M);
+        h[S::lane_of(sub, l)] = 0;
+      }
+    } else {
+      gather_sum_staged<B, FE, L>(st, my_a - beg, my_e - beg, P.X, sub, M, acc);
+    }
+    const uint32_t s1 = P.scale[r];
+    uint32_t o[LPT];
+    if (MODE == kModeOdd) {  // U = d_r z = redc(t * d_r R^2), t = z R^{-1}
+#pragma unroll
+      for (int l = 0; l < LPT; ++l) o[l] = redc((uint64_t)redc(acc[l], M) * s1, M);
+    } else {  // w' = redc(t * d_c R^2); x' = d_c w' = redc(w' * d_c R)
+      const uint32_t s2 = P.scale2[r];
+#pragma unroll
+      for (int l = 0; l < LPT; ++l) o[l] = redc((uint64_t)redc((uint64_t)redc(acc[l], M) * s1, M) * s2, M);
+    }
+#pragma unroll
+    for (int v = 0; v < NV; ++v)
+      P.Y[r * (B / 4) + S::word_of(sub, v)] = make_uint4(o[4 * v], o[4 * v + 1], o[4 * v + 2], o[4 * v + 3]);
+  }
+}
+
 // Lanes per thread of the single-matrix odd and even passes: 4 (a whole
 // 16-lane row in one warp load instruction, one L1 line look-up per gathered
 // row) at padded width 16, the pass kernels' default otherwise.
 template <int B>
 constexpr int kLeanLpt = (B == 16) ? 4 : kDefaultLpt<B>;
+
+// The single-matrix odd / even pass kernel: staged CSR entries (B >= 8), or
+// the plain pass kernel without Gram terms at B = 4 (32 rows per warp batch).
+template <int B, int MODE, int FE>
+constexpr void (*lean_kernel())(PassParams) {
+  if constexpr (B >= 8) return staged_pass_kernel<B, kLeanLpt<B>, MODE, FE>;
+  else return pass_kernel<B, MODE, FE, false, kLeanLpt<B>>;
+}
 
 // ---------------------------------------------------------------- Gram pass on tcgen05
 // The Gram term of a block (kModeGram: gz = x * scale, gu = gram_sym ? gz : x
@@ -700,41 +811,23 @@ struct TcShape {
   static constexpr int MR = 4 * B;              // real A rows (limb, lane)
   static constexpr int M = 128;                 // UMMA M (zero rows above MR)
   static constexpr int N = 4 * B;               // UMMA N
-  static constexpr int A_BYTES = M * kTcRows;   // per buffer
+  static constexpr int A_BYTES = M * kTcRows;   // per operand buffer
   static constexpr int B_BYTES = N * kTcRows;
-  static constexpr int COLS = N <= 64 ? 64 : 128;  // TMEM columns allocated
+  static constexpr int OPS_BYTES = 2 * (A_BYTES + B_BYTES);  // two operand buffers
+  static constexpr int RAW_Y = kTcRows * B * 4;              // a tile's block rows
+  static constexpr int RAW_BYTES = RAW_Y + kTcRows * 4;      // plus its row scales
+  static constexpr int RING = B >= 32 ? 2 : 4;               // raw tiles in flight
+  static constexpr int COLS = N <= 64 ? 64 : 128;            // TMEM columns allocated
   static constexpr uint32_t IDESC = (2u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 };
 
 template <int B>
 constexpr size_t gram_tc_smem_bytes() {
-  return 2 * (size_t)(TcShape<B>::A_BYTES + TcShape<B>::B_BYTES);
+  return (size_t)TcShape<B>::OPS_BYTES + (size_t)TcShape<B>::RING * TcShape<B>::RAW_BYTES;
 }
-
-// One staging task: 4 consecutive rows x 4 lanes (one 128-bit word per row)
-// of the block and the 4 row scales, loaded a tile ahead.
-template <int B>
-struct TcLoad {
-  static constexpr int GROUPS = B / 4;                    // 128-bit words per row
-  static constexpr int TASKS = (kTcRows / 4) * GROUPS;    // per tile
-  static constexpr int TPT = TASKS / kThreads;            // per thread
-  uint4 y[TPT][4];
-  uint32_t sc[TPT][4];
-  __device__ __forceinline__ void load(const PassParams& P, int64_t tile, int tid) {
-#pragma unroll
-    for (int t = 0; t < TPT; ++t) {
-      const int task = tid + t * kThreads, g = task % GROUPS, qd = task / GROUPS;
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int64_t r = tile * kTcRows + 4 * qd + q;
-        const bool in = r < P.rows;
-        y[t][q] = in ? __ldg(P.X + r * GROUPS + g) : make_uint4(0, 0, 0, 0);
-        sc[t][q] = in ? __ldg(P.scale + r) : 0u;
-      }
-    }
-  }
-};
-static_assert(TcLoad<16>::TASKS % kThreads == 0 && TcLoad<32>::TASKS % kThreads == 0, "staging tasks");
+// dynamic + static (the CTA sums) within the 227 KB a CTA may hold
+static_assert(gram_tc_smem_bytes<16>() + 16 * 16 * 8 + 1024 <= 232448, "Gram tile ring too large");
+static_assert(gram_tc_smem_bytes<32>() + 32 * 32 * 8 + 1024 <= 232448, "Gram tile ring too large");
 
 __device__ __forceinline__ void byte_transpose4(const uint32_t (&v)[4], uint32_t (&w)[4]) {
   // w[a] = bytes a of v[0..3]: limb a of four consecutive rows
@@ -746,28 +839,55 @@ __device__ __forceinline__ void byte_transpose4(const uint32_t (&v)[4], uint32_t
   w[3] = __byte_perm(t2, t3, 0x7632);
 }
 
+// Thread 0: the raw rows (and scales) of `tile` into ring slot `dst` by two
+// 1-D bulk copies completing on `mbar` (rows past the end are not copied; the
+// scale copy is rounded up to 16 bytes, which the scale arrays are padded for).
 template <int B>
-__global__ void __launch_bounds__(kThreads, (B >= 32 ? 1 : 2)) gram_tc_kernel(PassParams P, int* status) {
+__device__ __forceinline__ void tc_fetch(const PassParams& P, int64_t tile, unsigned char* dst, uint64_t* mbar) {
+  using T = TcShape<B>;
+  const int64_t r0 = tile * kTcRows;
+  const int rows = (int)(P.rows - r0 < kTcRows ? P.rows - r0 : kTcRows);
+  const uint32_t ybytes = (uint32_t)rows * B * 4;
+  const uint32_t sbytes = (uint32_t)((rows * 4 + 15) & ~15);
+  const uint32_t mb = smem_u32(mbar);
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(ybytes + sbytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(reinterpret_cast<const uint32_t*>(P.X) + r0 * B), "r"(ybytes), "r"(mb)
+               : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst + T::RAW_Y)),
+               "l"(P.scale + r0), "r"(sbytes), "r"(mb)
+               : "memory");
+}
+
+template <int B>
+__global__ void __launch_bounds__(kThreads, 1) gram_tc_kernel(PassParams P, int* status) {
   using T = TcShape<B>;
   constexpr int NP = B * (B + 1) / 2;
+  constexpr int GROUPS = B / 4;                       // 128-bit words per row
+  constexpr int TASKS = (kTcRows / 4) * GROUPS;       // 4 rows x 4 lanes each
   extern __shared__ __align__(1024) unsigned char tc_smem[];
-  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ __align__(8) uint64_t mbar[2];           // MMA completion per operand buffer
+  __shared__ __align__(8) uint64_t rbar[T::RING];     // bulk-copy completion per raw slot
   __shared__ uint32_t tmem_base_s;
   __shared__ unsigned long long red[B * B];
   __shared__ bool is_last;
   __shared__ int s_fail;
-  // buffer s: A at tc_smem + s (A + B bytes), B right after it
+  unsigned char* const raw0 = tc_smem + T::OPS_BYTES;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const ModP M = P.M;
 
-  // zero both buffers once (the A rows above 4B stay zero), the CTA sums, the barriers
-  for (int e = tid; e < (int)(gram_tc_smem_bytes<B>() / 16); e += kThreads)
-    reinterpret_cast<uint4*>(tc_smem)[e] = make_uint4(0, 0, 0, 0);
+  // zero the operand buffers once (the A rows above 4B stay zero), the CTA sums, the barriers
+  for (int e = tid; e < T::OPS_BYTES / 16; e += kThreads) reinterpret_cast<uint4*>(tc_smem)[e] = make_uint4(0, 0, 0, 0);
   for (int e = tid; e < B * B; e += kThreads) red[e] = 0;
   if (tid == 0) {
     s_fail = 0;
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])) : "memory");
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])) : "memory");
+    for (int i = 0; i < 2; ++i)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[i])) : "memory");
+    for (int i = 0; i < T::RING; ++i)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&rbar[i])) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)),
@@ -779,6 +899,14 @@ __global__ void __launch_bounds__(kThreads, (B >= 32 ? 1 : 2)) gram_tc_kernel(Pa
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_base_s;
+
+  const int64_t ntiles = (P.rows + kTcRows - 1) / kTcRows;
+  const int64_t mine = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;  // tiles of this CTA
+  if (tid == 0) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    for (int64_t j = 0; j < mine && j < T::RING; ++j)
+      tc_fetch<B>(P, blockIdx.x + j * gridDim.x, raw0 + j * T::RAW_BYTES, &rbar[j]);
+  }
 
   // per-thread sums of the drained limb products: thread (warp w < 4, lane l)
   // owns A row m = 32 w + l = (a, i) and keeps sum_c 256^{a+c} D[m][(c, j)] mod p per j
@@ -797,12 +925,11 @@ __global__ void __launch_bounds__(kThreads, (B >= 32 ? 1 : 2)) gram_tc_kernel(Pa
       w = w * 256 % M.p;
     }
   }
-  // drain: wait for every committed MMA, add D into part[], restart accumulation
   uint32_t commits[2] = {0, 0};
   auto drain = [&]() {
     if (tid == 0) {
-      for (int s = 0; s < 2; ++s)
-        if (commits[s] && !mbar_wait(smem_u32(&mbar[s]), (commits[s] - 1) & 1)) {
+      for (int q = 0; q < 2; ++q)
+        if (commits[q] && !mbar_wait(smem_u32(&mbar[q]), (commits[q] - 1) & 1)) {
           s_fail = 1;
           atomicExch(status, 1);
         }
@@ -834,39 +961,50 @@ __global__ void __launch_bounds__(kThreads, (B >= 32 ? 1 : 2)) gram_tc_kernel(Pa
     __syncthreads();
   };
 
-  const int64_t ntiles = (P.rows + kTcRows - 1) / kTcRows;
-  int64_t tl = 0;        // tiles of this CTA so far
   bool acc_live = false;  // D holds sums to accumulate onto
-  TcLoad<B> cur;
-  if ((int64_t)blockIdx.x < ntiles) cur.load(P, blockIdx.x, tid);
-  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++tl) {
-    const int s = (int)(tl & 1);
+  int64_t jstop = mine;   // the tile at which a wait gave up
+  for (int64_t j = 0; j < mine; ++j) {
+    const int slot = (int)(j % T::RING), s = (int)(j & 1);
+    unsigned char* const raw = raw0 + slot * T::RAW_BYTES;
     unsigned char* const bufA = tc_smem + s * (T::A_BYTES + T::B_BYTES);
     unsigned char* const bufB = bufA + T::A_BYTES;
-    if (tl >= 2) {  // the MMAs of tile tl - 2 read this buffer
-      if (tid == 0 && !mbar_wait(smem_u32(&mbar[s]), (commits[s] - 1) & 1)) {
-        s_fail = 1;
-        atomicExch(status, 1);
-      }
-      __syncthreads();
+    // the raw tile has landed (every thread polls the barrier) and the MMAs
+    // of tile j - 2 no longer read operand buffer s
+    if (!mbar_wait(smem_u32(&rbar[slot]), (uint32_t)((j / T::RING) & 1))) {
+      s_fail = 1;
+      atomicExch(status, 1);
     }
-    if (s_fail) break;
-    // stage the tile loaded a round ago, with the next tile's loads already in flight
-    TcLoad<B> nxt;
-    if (tile + gridDim.x < ntiles) nxt.load(P, tile + gridDim.x, tid);
+    if (j >= 2 && tid == 0 && !mbar_wait(smem_u32(&mbar[s]), (commits[s] - 1) & 1)) {
+      s_fail = 1;
+      atomicExch(status, 1);
+    }
+    __syncthreads();
+    if (s_fail) {
+      jstop = j;
+      break;
+    }
+    const int64_t r0 = (blockIdx.x + j * gridDim.x) * kTcRows;
+    const uint32_t* scl = reinterpret_cast<const uint32_t*>(raw + T::RAW_Y);
+    for (int task = tid; task < TASKS; task += kThreads) {
+      const int g = task % GROUPS, qd = task / GROUPS;
+      uint4 y[4];
+      uint32_t sc[4];
 #pragma unroll
-    for (int t = 0; t < TcLoad<B>::TPT; ++t) {
-      const int task = tid + t * kThreads, g = task % TcLoad<B>::GROUPS, qd = task / TcLoad<B>::GROUPS;
+      for (int q = 0; q < 4; ++q) {
+        const int rr = 4 * qd + q;
+        const bool in = r0 + rr < P.rows;
+        y[q] = in ? *reinterpret_cast<const uint4*>(raw + ((size_t)rr * B + 4 * g) * 4) : make_uint4(0, 0, 0, 0);
+        sc[q] = in ? scl[rr] : 0u;
+      }
 #pragma unroll
       for (int c4 = 0; c4 < 4; ++c4) {
         const int i = 4 * g + c4;
         uint32_t z[4], u[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          const uint4 y4 = cur.y[t][q];
-          const uint32_t y = c4 == 0 ? y4.x : c4 == 1 ? y4.y : c4 == 2 ? y4.z : y4.w;
-          z[q] = redc((uint64_t)y * cur.sc[t][q], M);
-          u[q] = P.gram_sym ? z[q] : y;
+          const uint32_t yv = c4 == 0 ? y[q].x : c4 == 1 ? y[q].y : c4 == 2 ? y[q].z : y[q].w;
+          z[q] = redc((uint64_t)yv * sc[q], M);
+          u[q] = P.gram_sym ? z[q] : yv;
         }
         uint32_t wz[4], wu[4];
         byte_transpose4(z, wz);
@@ -878,9 +1016,8 @@ __global__ void __launch_bounds__(kThreads, (B >= 32 ? 1 : 2)) gram_tc_kernel(Pa
         }
       }
     }
-    cur = nxt;
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
+    __syncthreads();  // operand buffer s written, raw slot read by every thread
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint32_t a0 = smem_u32(bufA), b0 = smem_u32(bufB);
@@ -900,19 +1037,25 @@ __global__ void __launch_bounds__(kThreads, (B >= 32 ? 1 : 2)) gram_tc_kernel(Pa
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                        smem_u32(&mbar[s]))
                    : "memory");
+      // refill the raw slot just read with the tile RING ahead
+      if (j + T::RING < mine) tc_fetch<B>(P, blockIdx.x + (j + T::RING) * gridDim.x, raw, &rbar[slot]);
     }
     commits[s] += 1;
     acc_live = true;
-    if ((tl + 1) % kTcDrain == 0) {
+    if ((j + 1) % kTcDrain == 0) {
       drain();
       acc_live = false;
     }
   }
   if (acc_live && !s_fail) drain();
-  if (s_fail) {  // let what was committed finish before the memory goes away
-    if (tid == 0)
-      for (int s = 0; s < 2; ++s)
-        if (commits[s]) mbar_wait(smem_u32(&mbar[s]), (commits[s] - 1) & 1);
+  if (s_fail) {  // let what was committed or fetched finish before the memory goes away
+    if (tid == 0) {
+      for (int q = 0; q < 2; ++q)
+        if (commits[q]) mbar_wait(smem_u32(&mbar[q]), (commits[q] - 1) & 1);
+      // fetches still unconsumed: tiles [jstop, min(mine, jstop + RING)), one per slot
+      for (int64_t j = jstop; j < mine && j < jstop + T::RING; ++j)
+        mbar_wait(smem_u32(&rbar[(int)(j % T::RING)]), (uint32_t)((j / T::RING) & 1));
+    }
     __syncthreads();
   }
   if (warp == 0) {
@@ -923,14 +1066,14 @@ __global__ void __launch_bounds__(kThreads, (B >= 32 ? 1 : 2)) gram_tc_kernel(Pa
   if (reader) {
     const int i = m_row % B;
 #pragma unroll
-    for (int j = 0; j < B; ++j) atomicAdd(&red[i * B + j], (unsigned long long)part[j]);
+    for (int jj = 0; jj < B; ++jj) atomicAdd(&red[i * B + jj], (unsigned long long)part[jj]);
   }
   __syncthreads();
   unsigned long long* const acc = P.gram_acc + (size_t)(blockIdx.x % P.replicas) * P.gram_stride;
   for (int q = tid; q < NP; q += kThreads) {
-    int i, j;
-    pair_of(q, B, i, j);
-    atomicAdd(&acc[q], (unsigned long long)reduce(red[i * B + j], M));
+    int i, jj;
+    pair_of(q, B, i, jj);
+    atomicAdd(&acc[q], (unsigned long long)reduce(red[i * B + jj], M));
   }
   __threadfence();
   __syncthreads();
@@ -943,9 +1086,9 @@ __global__ void __launch_bounds__(kThreads, (B >= 32 ? 1 : 2)) gram_tc_kernel(Pa
   const int npr = b * (b + 1) / 2;
   uint32_t* S_out = *P.S_ptr + (size_t)__ldcg(P.term_ctr) * npr;
   for (int q = tid; q < npr; q += kThreads) {
-    int i, j;
-    pair_of(q, b, i, j);
-    const int qb = pair_index(i, j, B);
+    int i, jj;
+    pair_of(q, b, i, jj);
+    const int qb = pair_index(i, jj, B);
     unsigned long long v = 0;
     for (int r = 0; r < P.replicas; ++r) v += __ldcg(P.gram_acc + (size_t)r * P.gram_stride + qb);
     S_out[q] = mulmod(reduce(v, M), P.gram_mul, M);
@@ -1178,8 +1321,8 @@ static int launch_pass_BF(rr_krylov* kr, const PassParams& P, int mode, dim3 gri
   const size_t sm = pass_smem_bytes<B>();
   switch (mode) {
     case kModeInit: return launch_ex(kr, pass_kernel<B, kModeInit, FE, true>, grid, block, sm, s, P);
-    case kModeOdd: return launch_ex(kr, pass_kernel<B, kModeOdd, FE, false, kLeanLpt<B>>, grid, block, 0, s, P);
-    case kModeEven: return launch_ex(kr, pass_kernel<B, kModeEven, FE, false, kLeanLpt<B>>, grid, block, 0, s, P);
+    case kModeOdd: return launch_ex(kr, lean_kernel<B, kModeOdd, FE>(), grid, block, 0, s, P);
+    case kModeEven: return launch_ex(kr, lean_kernel<B, kModeEven, FE>(), grid, block, 0, s, P);
     default: return launch_ex(kr, pass_kernel<B, kModeGram, FE, true>, grid, block, sm, s, P);
   }
 }
@@ -1188,8 +1331,7 @@ static int launch_pass_BF(rr_krylov* kr, const PassParams& P, int mode, dim3 gri
 template <int B>
 static int launch_gram_tc(rr_krylov* kr, const PassParams& P, cudaStream_t s) {
   const int64_t ntiles = (P.rows + kTcRows - 1) / kTcRows;
-  const int per_sm = B >= 32 ? 1 : 2;
-  const dim3 grid((unsigned)std::max<int64_t>(1, std::min<int64_t>(ntiles, per_sm * (int64_t)kr->mat->ctx->num_sms)));
+  const dim3 grid((unsigned)std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)kr->mat->ctx->num_sms)));
   return launch_ex(kr, gram_tc_kernel<B>, grid, dim3(kThreads), gram_tc_smem_bytes<B>(), s, P,
                         kr->d_status.ptr);
 }
@@ -1254,14 +1396,12 @@ static int occupancy_B(rr_krylov* kr, int* pass_blocks, int* chunk_blocks, int* 
     RR_TRY((set_pass_smem<B, 4>()));
     RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(pass_blocks, pass_kernel<B, kModeGram, 4>, kThreads, sm));
     RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(chunk_blocks, chunk_kernel<B, 4>, kThreads, 0));
-    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(lean_blocks, pass_kernel<B, kModeOdd, 4, false, kLeanLpt<B>>,
-                                                          kThreads, 0));
+    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(lean_blocks, lean_kernel<B, kModeOdd, 4>(), kThreads, 0));
   } else {
     RR_TRY((set_pass_smem<B, 2>()));
     RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(pass_blocks, pass_kernel<B, kModeGram, 2>, kThreads, sm));
     RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(chunk_blocks, chunk_kernel<B, 2>, kThreads, 0));
-    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(lean_blocks, pass_kernel<B, kModeOdd, 2, false, kLeanLpt<B>>,
-                                                          kThreads, 0));
+    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(lean_blocks, lean_kernel<B, kModeOdd, 2>(), kThreads, 0));
   }
   return RR_OK;
 }
