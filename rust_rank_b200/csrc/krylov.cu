@@ -472,7 +472,7 @@ __device__ __forceinline__ void pass_body(const PassParams& P, uint32_t* gram_sm
     uint32_t gz[LPT], gu[LPT];
     if (r < P.rows) {
       uint32_t t[LPT];
-      if (MODE == kModeInit || MODE == kModeGram) {
+      if (MODE == kModeInit) {
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
           const uint4 w = ld_block<COH>(P.X + r * (B / 4) + S::word_of(sub, v));
@@ -514,14 +514,6 @@ __device__ __forceinline__ void pass_body(const PassParams& P, uint32_t* gram_sm
           gu[l] = gz[l];
           o[l] = redc((uint64_t)gz[l] * s2, M);
         }
-      } else if (MODE == kModeGram) {
-        // gz = x * d^{-1} (scale = d^{-1} R); gu = gz or x
-#pragma unroll
-        for (int l = 0; l < LPT; ++l) {
-          gz[l] = redc((uint64_t)t[l] * s1, M);
-          gu[l] = P.gram_sym ? gz[l] : t[l];
-          o[l] = 0;
-        }
       } else {
         // init: w given; x = d_c w = redc(w * d_c R)
 #pragma unroll
@@ -531,11 +523,9 @@ __device__ __forceinline__ void pass_body(const PassParams& P, uint32_t* gram_sm
           o[l] = redc((uint64_t)t[l] * s1, M);
         }
       }
-      if (MODE != kModeGram) {
 #pragma unroll
-        for (int v = 0; v < NV; ++v)
-          P.Y[r * (B / 4) + S::word_of(sub, v)] = make_uint4(o[4 * v], o[4 * v + 1], o[4 * v + 2], o[4 * v + 3]);
-      }
+      for (int v = 0; v < NV; ++v)
+        P.Y[r * (B / 4) + S::word_of(sub, v)] = make_uint4(o[4 * v], o[4 * v + 1], o[4 * v + 2], o[4 * v + 3]);
     } else {
 #pragma unroll
       for (int l = 0; l < LPT; ++l) { gz[l] = 0; gu[l] = 0; }
@@ -630,122 +620,20 @@ __global__ void __launch_bounds__(kThreads, (B >= 32 && GRAM ? 2 : 4)) pass_kern
   pass_body<B, MODE, FE, false, GRAM, L>(P, gram_smem, red, is_last);
 }
 
-// ---------------------------------------------------------------- staged single-matrix passes
-// The odd and even passes of the single-matrix path without Gram terms, with
-// each warp batch's CSR entries staged in shared memory first: the batch's
-// rows are consecutive, so their entries are one contiguous run that the warp
-// copies with coalesced loads (32 entries per instruction), and every thread
-// then reads its row's entries from shared memory.  Loading the entries
-// straight from global memory costs one L1 look-up per entry per row (the
-// rows of a warp batch lie in different lines); staged, a batch's entries
-// cost a handful of look-ups, and the L1 pipe is left to the gathers.  Rows
-// longer than kHeavyDegree take their sums from heavy_acc (chunk kernel), so
-// a batch stages at most RPW * kHeavyDegree entries.
-template <int B, int FE, int L>
-__device__ __forceinline__ void gather_sum_staged(const uint2* st, uint32_t beg, uint32_t end,
-                                                  const uint4* __restrict__ X, int sub, const ModP& M,
-                                                  uint64_t (&acc)[Shape<B, L>::LPT]) {
-  constexpr int NV = Shape<B, L>::NV, TPR = Shape<B, L>::TPR;
-  constexpr int RW = B / 4;
-  const uint4* Xs = X + sub;
-  uint32_t k = beg;
-  for (; k + 3 < end; k += 4) {
-    uint2 e[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) e[u] = st[k + u];
-    uint4 g[4][NV];
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-#pragma unroll
-      for (int v = 0; v < NV; ++v) g[u][v] = __ldg(Xs + (size_t)e[u].x * RW + v * TPR);
-    mac_step<B, FE, L>(e, g, M, acc);
-  }
-  if (k < end) {
-    uint2 e[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      e[u] = st[k + u < end ? k + u : k];
-      if (k + u >= end) e[u].y = 0u;
-    }
-    uint4 g[4][NV];
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-#pragma unroll
-      for (int v = 0; v < NV; ++v) g[u][v] = __ldg(Xs + (size_t)e[u].x * RW + v * TPR);
-    mac_step<B, FE, L>(e, g, M, acc);
-  }
-}
-
-template <int B, int L, int MODE, int FE>
-__global__ void __launch_bounds__(kThreads, 4) staged_pass_kernel(PassParams P) {
-  using S = Shape<B, L>;
-  constexpr int LPT = S::LPT, NV = S::NV, TPR = S::TPR, RPW = S::RPW;
-  constexpr int CAP = RPW * (int)kHeavyDegree;
-  static_assert(RPW < 32, "row offsets of a batch are held one per lane");
-  __shared__ uint2 stage_all[kWarps][CAP];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int sub = lane % TPR, slot = lane / TPR;
-  uint2* const st = stage_all[warp];
-  const ModP M = P.M;
-  const int64_t nbatch = (P.rows + RPW - 1) / RPW;
-  const int64_t nw = (int64_t)gridDim.x * kWarps;
-  for (int64_t batch = (int64_t)blockIdx.x * kWarps + warp; batch < nbatch; batch += nw) {
-    const int64_t r0 = batch * RPW;
-    const int64_t rlast = r0 + RPW < P.rows ? r0 + RPW : P.rows;
-    uint32_t off = 0;  // lane j <= RPW: rowptr[r0 + j] (clamped to the last row)
-    if (lane <= RPW) off = P.rowptr[r0 + lane < rlast ? r0 + lane : rlast];
-    const int64_t rs = r0 > P.heavy_rows ? r0 : (P.heavy_rows < rlast ? P.heavy_rows : rlast);
-    const uint32_t beg = __shfl_sync(0xffffffffu, off, (int)(rs - r0));
-    const uint32_t end = __shfl_sync(0xffffffffu, off, (int)(rlast - r0));
-    const uint32_t my_a = __shfl_sync(0xffffffffu, off, slot);
-    const uint32_t my_e = __shfl_sync(0xffffffffu, off, slot + 1);
-    __syncwarp();  // the previous batch has finished reading st
-    for (uint32_t k = lane; k < end - beg; k += 32) st[k] = __ldg(P.cv + beg + k);
-    __syncwarp();
-    const int64_t r = r0 + slot;
-    if (r >= P.rows) continue;
-    uint64_t acc[LPT];
-#pragma unroll
-    for (int l = 0; l < LPT; ++l) acc[l] = 0;
-    if (r < P.heavy_rows) {
-      unsigned long long* h = P.heavy_acc + (size_t)r * B;
-#pragma unroll
-      for (int l = 0; l < LPT; ++l) {
-        acc[l] = fold(h[S::lane_of(sub, l)], M);
-        h[S::lane_of(sub, l)] = 0;
-      }
-    } else {
-      gather_sum_staged<B, FE, L>(st, my_a - beg, my_e - beg, P.X, sub, M, acc);
-    }
-    const uint32_t s1 = P.scale[r];
-    uint32_t o[LPT];
-    if (MODE == kModeOdd) {  // U = d_r z = redc(t * d_r R^2), t = z R^{-1}
-#pragma unroll
-      for (int l = 0; l < LPT; ++l) o[l] = redc((uint64_t)redc(acc[l], M) * s1, M);
-    } else {  // w' = redc(t * d_c R^2); x' = d_c w' = redc(w' * d_c R)
-      const uint32_t s2 = P.scale2[r];
-#pragma unroll
-      for (int l = 0; l < LPT; ++l) o[l] = redc((uint64_t)redc((uint64_t)redc(acc[l], M) * s1, M) * s2, M);
-    }
-#pragma unroll
-    for (int v = 0; v < NV; ++v)
-      P.Y[r * (B / 4) + S::word_of(sub, v)] = make_uint4(o[4 * v], o[4 * v + 1], o[4 * v + 2], o[4 * v + 3]);
-  }
-}
-
 // Lanes per thread of the single-matrix odd and even passes: 4 (a whole
 // 16-lane row in one warp load instruction, one L1 line look-up per gathered
 // row) at padded width 16, the pass kernels' default otherwise.
 template <int B>
-constexpr int kLeanLpt = (B == 16) ? 4 : kDefaultLpt<B>;
+constexpr int kLeanLpt = (B >= 16) ? 4 : kDefaultLpt<B>;
 
-// The single-matrix odd / even pass kernel: staged CSR entries (B >= 8), or
-// the plain pass kernel without Gram terms at B = 4 (32 rows per warp batch).
-template <int B, int MODE, int FE>
-constexpr void (*lean_kernel())(PassParams) {
-  if constexpr (B >= 8) return staged_pass_kernel<B, kLeanLpt<B>, MODE, FE>;
-  else return pass_kernel<B, MODE, FE, false, kLeanLpt<B>>;
-}
+// Padded widths whose single-matrix odd and even passes compute their Gram
+// terms themselves (u8-limb mma.sync on the block rows still in registers);
+// at width 32 the passes run without Gram terms and a tcgen05 Gram pass
+// (gram_tc_kernel) reads each written block once more.  Measured on the 2M x
+// 1.5M Zipf matrix: fused 0.63 ms per application at width 16 against 0.69
+// split; split 1.11 ms at width 32 against 1.29 fused.
+template <int B>
+constexpr bool kFusedGram = (B <= 16);
 
 // ---------------------------------------------------------------- Gram pass on tcgen05
 // The Gram term of a block (kModeGram: gz = x * scale, gu = gram_sym ? gz : x
@@ -779,6 +667,15 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
          (1ull << 46);
 }
 
+// Operand rows within a limb: lane i = 4 g + c (g its 128-bit word, c the
+// word's component) sits in row c * B/4 + g, so that the 32 stores of one
+// warp instruction (8 words g x 4 row quads, fixed c) fall in 32 different
+// banks at B = 32.  tc_lane maps a row back to its lane.
+template <int B>
+__device__ __forceinline__ constexpr int tc_lane(int r) {
+  return 4 * (r % (B / 4)) + r / (B / 4);
+}
+
 // Byte offset of (row, k) in a staged operand of R rows x 128 K-bytes.
 __device__ __forceinline__ uint32_t tc_off(int R, int row, int k) {
   return (uint32_t)((k >> 5) * (R / 8) * 256 + (row >> 3) * 256 + ((k & 31) >> 4) * 128 + (row & 7) * 16 + (k & 15));
@@ -805,6 +702,8 @@ __device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity) {
     if (tc_ns() - t0 > kTcWaitLimitNs) return false;
   }
 }
+
+constexpr int kTcThreads = 512;  // Gram pass CTA: 16 warps, one CTA per SM
 
 template <int B>
 struct TcShape {
@@ -862,7 +761,7 @@ __device__ __forceinline__ void tc_fetch(const PassParams& P, int64_t tile, unsi
 }
 
 template <int B>
-__global__ void __launch_bounds__(kThreads, 1) gram_tc_kernel(PassParams P, int* status) {
+__global__ void __launch_bounds__(kTcThreads, 1) gram_tc_kernel(PassParams P, int* status) {
   using T = TcShape<B>;
   constexpr int NP = B * (B + 1) / 2;
   constexpr int GROUPS = B / 4;                       // 128-bit words per row
@@ -879,8 +778,8 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc_kernel(PassParams P, int*
   const ModP M = P.M;
 
   // zero the operand buffers once (the A rows above 4B stay zero), the CTA sums, the barriers
-  for (int e = tid; e < T::OPS_BYTES / 16; e += kThreads) reinterpret_cast<uint4*>(tc_smem)[e] = make_uint4(0, 0, 0, 0);
-  for (int e = tid; e < B * B; e += kThreads) red[e] = 0;
+  for (int e = tid; e < T::OPS_BYTES / 16; e += kTcThreads) reinterpret_cast<uint4*>(tc_smem)[e] = make_uint4(0, 0, 0, 0);
+  for (int e = tid; e < B * B; e += kTcThreads) red[e] = 0;
   if (tid == 0) {
     s_fail = 0;
     for (int i = 0; i < 2; ++i)
@@ -909,7 +808,8 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc_kernel(PassParams P, int*
   }
 
   // per-thread sums of the drained limb products: thread (warp w < 4, lane l)
-  // owns A row m = 32 w + l = (a, i) and keeps sum_c 256^{a+c} D[m][(c, j)] mod p per j
+  // owns A row m = 32 w + l = (a, i) (tc_row) and keeps
+  // sum_c 256^{a+c} D[m][(c, j)] mod p per j
   uint32_t part[B];
 #pragma unroll
   for (int j = 0; j < B; ++j) part[j] = 0;
@@ -951,7 +851,7 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc_kernel(PassParams P, int*
         if (reader) {
 #pragma unroll
           for (int q = 0; q < 16; ++q) {
-            const int n = c0 + q, c = n / B, j = n % B;
+            const int n = c0 + q, c = n / B, j = tc_lane<B>(n % B);
             part[j] = addmod(part[j], mulmod(v[q], wgt[c], M), M.p);
           }
         }
@@ -985,7 +885,7 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc_kernel(PassParams P, int*
     }
     const int64_t r0 = (blockIdx.x + j * gridDim.x) * kTcRows;
     const uint32_t* scl = reinterpret_cast<const uint32_t*>(raw + T::RAW_Y);
-    for (int task = tid; task < TASKS; task += kThreads) {
+    for (int task = tid; task < TASKS; task += kTcThreads) {
       const int g = task % GROUPS, qd = task / GROUPS;
       uint4 y[4];
       uint32_t sc[4];
@@ -997,8 +897,7 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc_kernel(PassParams P, int*
         sc[q] = in ? scl[rr] : 0u;
       }
 #pragma unroll
-      for (int c4 = 0; c4 < 4; ++c4) {
-        const int i = 4 * g + c4;
+      for (int c4 = 0; c4 < 4; ++c4) {  // lane 4 g + c4
         uint32_t z[4], u[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
@@ -1011,8 +910,8 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc_kernel(PassParams P, int*
         byte_transpose4(u, wu);
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
-          *reinterpret_cast<uint32_t*>(bufA + tc_off(T::M, a * B + i, 4 * qd)) = wz[a];
-          *reinterpret_cast<uint32_t*>(bufB + tc_off(T::N, a * B + i, 4 * qd)) = wu[a];
+          *reinterpret_cast<uint32_t*>(bufA + tc_off(T::M, a * B + c4 * GROUPS + g, 4 * qd)) = wz[a];
+          *reinterpret_cast<uint32_t*>(bufB + tc_off(T::N, a * B + c4 * GROUPS + g, 4 * qd)) = wu[a];
         }
       }
     }
@@ -1064,13 +963,13 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc_kernel(PassParams P, int*
   }
   // CTA sums: G[i][j] += part (4 limb rows a per (i, j))
   if (reader) {
-    const int i = m_row % B;
+    const int i = tc_lane<B>(m_row % B);
 #pragma unroll
     for (int jj = 0; jj < B; ++jj) atomicAdd(&red[i * B + jj], (unsigned long long)part[jj]);
   }
   __syncthreads();
   unsigned long long* const acc = P.gram_acc + (size_t)(blockIdx.x % P.replicas) * P.gram_stride;
-  for (int q = tid; q < NP; q += kThreads) {
+  for (int q = tid; q < NP; q += kTcThreads) {
     int i, jj;
     pair_of(q, B, i, jj);
     atomicAdd(&acc[q], (unsigned long long)reduce(red[i * B + jj], M));
@@ -1085,7 +984,7 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc_kernel(PassParams P, int*
   const int b = P.b_real;
   const int npr = b * (b + 1) / 2;
   uint32_t* S_out = *P.S_ptr + (size_t)__ldcg(P.term_ctr) * npr;
-  for (int q = tid; q < npr; q += kThreads) {
+  for (int q = tid; q < npr; q += kTcThreads) {
     int i, jj;
     pair_of(q, b, i, jj);
     const int qb = pair_index(i, jj, B);
@@ -1094,7 +993,7 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc_kernel(PassParams P, int*
     S_out[q] = mulmod(reduce(v, M), P.gram_mul, M);
   }
   __syncthreads();
-  for (int q = tid; q < NP * P.replicas; q += kThreads)
+  for (int q = tid; q < NP * P.replicas; q += kTcThreads)
     __stcg(P.gram_acc + (size_t)(q / NP) * P.gram_stride + q % NP, 0ull);
   if (tid == 0) {
     *P.term_ctr += 1u;
@@ -1183,10 +1082,16 @@ __global__ void barrier_check_kernel(unsigned int* bar, int* error, uint64_t lim
 // Long rows: one warp per chunk of at most kChunkNnz entries.  Lanes form RPW
 // slots of TPR threads; slot s takes entries beg+s, beg+s+RPW, ...  The slot
 // sums (exact residues) are combined with shuffles and added to heavy_acc with
-// 64-bit atomics.
-template <int B, int FE>
+// 64-bit atomics.  L = 4 lanes per thread at widths 16 and 32: each gathered
+// row is read whole by one warp load instruction (64 or 128 bytes), so the
+// L1 data pipe handles half as many wavefronts per gathered byte as with rows
+// split over two instructions.
+template <int B>
+constexpr int kChunkLpt = (B >= 16) ? 4 : kDefaultLpt<B>;
+
+template <int B, int FE, int L = kChunkLpt<B>>
 __global__ void __launch_bounds__(kThreads, 3) chunk_kernel(ChunkParams P) {
-  using S = Shape<B>;
+  using S = Shape<B, L>;
   constexpr int LPT = S::LPT, TPR = S::TPR, RPW = S::RPW;
   const int lane = threadIdx.x & 31;
   const int sub = lane % TPR;
@@ -1200,7 +1105,7 @@ __global__ void __launch_bounds__(kThreads, 3) chunk_kernel(ChunkParams P) {
     uint64_t acc[LPT];
 #pragma unroll
     for (int l = 0; l < LPT; ++l) acc[l] = 0;
-    gather_sum<B, FE>(P.cv, beg + slot, end, (uint32_t)RPW, P.X, sub, M, acc);
+    gather_sum<B, FE, false, L>(P.cv, beg + slot, end, (uint32_t)RPW, P.X, sub, M, acc);
     uint32_t y[LPT];
 #pragma unroll
     for (int l = 0; l < LPT; ++l) y[l] = reduce(acc[l], M);
@@ -1311,38 +1216,45 @@ static int launch_ex(const rr_krylov* kr, void (*fn)(Args...), dim3 grid, dim3 b
   return RR_OK;
 }
 
-// Single-matrix launches: the odd and even passes run without their Gram
-// terms (no staging, no tensor-core flush, so fewer registers and no shared
-// memory), each followed by a Gram pass over the block it wrote (kModeGram);
-// the initial pass computes S_0 itself.
+// Single-matrix launches: at widths up to 16 the odd and even passes add their
+// Gram terms themselves; at width 32 they run without them (no staging, no
+// tensor-core flush, so fewer registers and no shared memory), each followed
+// by a tcgen05 Gram pass over the block it wrote (kModeGram).  The initial
+// pass computes S_0 itself.
 template <int B, int FE>
 static int launch_pass_BF(rr_krylov* kr, const PassParams& P, int mode, dim3 grid, cudaStream_t s) {
   const dim3 block(kThreads);
   const size_t sm = pass_smem_bytes<B>();
   switch (mode) {
     case kModeInit: return launch_ex(kr, pass_kernel<B, kModeInit, FE, true>, grid, block, sm, s, P);
-    case kModeOdd: return launch_ex(kr, lean_kernel<B, kModeOdd, FE>(), grid, block, 0, s, P);
-    case kModeEven: return launch_ex(kr, lean_kernel<B, kModeEven, FE>(), grid, block, 0, s, P);
-    default: return launch_ex(kr, pass_kernel<B, kModeGram, FE, true>, grid, block, sm, s, P);
+    case kModeOdd:
+      if constexpr (kFusedGram<B>) return launch_ex(kr, pass_kernel<B, kModeOdd, FE, true>, grid, block, sm, s, P);
+      else return launch_ex(kr, pass_kernel<B, kModeOdd, FE, false, kLeanLpt<B>>, grid, block, 0, s, P);
+    case kModeEven:
+      if constexpr (kFusedGram<B>) return launch_ex(kr, pass_kernel<B, kModeEven, FE, true>, grid, block, sm, s, P);
+      else return launch_ex(kr, pass_kernel<B, kModeEven, FE, false, kLeanLpt<B>>, grid, block, 0, s, P);
   }
+  return fail(RR_EINVAL, "pass mode %d has no pass kernel at width %d", mode, B);
 }
 
-// Gram passes at padded widths 16 and 32 run on tcgen05 (gram_tc_kernel).
+// Gram passes at padded width 32 run on tcgen05 (gram_tc_kernel).
 template <int B>
 static int launch_gram_tc(rr_krylov* kr, const PassParams& P, cudaStream_t s) {
   const int64_t ntiles = (P.rows + kTcRows - 1) / kTcRows;
   const dim3 grid((unsigned)std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)kr->mat->ctx->num_sms)));
-  return launch_ex(kr, gram_tc_kernel<B>, grid, dim3(kThreads), gram_tc_smem_bytes<B>(), s, P,
+  return launch_ex(kr, gram_tc_kernel<B>, grid, dim3(kTcThreads), gram_tc_smem_bytes<B>(), s, P,
                         kr->d_status.ptr);
 }
 
 template <int B>
 static int launch_pass_B(rr_krylov* kr, const PassParams& P, int mode) {
-  if (mode == kModeGram && (B == 16 || B == 32)) {
-    cudaStream_t s = kr->launch_stream ? kr->launch_stream : kr->mat->ctx->stream;
-    return launch_gram_tc<(B >= 16 ? B : 16)>(kr, P, s);
+  if constexpr (B == 32) {
+    if (mode == kModeGram) {
+      cudaStream_t s = kr->launch_stream ? kr->launch_stream : kr->mat->ctx->stream;
+      return launch_gram_tc<32>(kr, P, s);
+    }
   }
-  const bool lean = mode == kModeOdd || mode == kModeEven;
+  const bool lean = !kFusedGram<B> && (mode == kModeOdd || mode == kModeEven);
   const dim3 grid(lean ? pass_grid_lean<B>(kr, P.rows) : pass_grid<B>(kr, P.rows));
   cudaStream_t s = kr->launch_stream ? kr->launch_stream : kr->mat->ctx->stream;
   return kr->fold4 ? launch_pass_BF<B, 4>(kr, P, mode, grid, s) : launch_pass_BF<B, 2>(kr, P, mode, grid, s);
@@ -1354,7 +1266,6 @@ static int set_pass_smem() {
   RR_CUDA(cudaFuncSetAttribute(pass_kernel<B, kModeInit, FE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
   RR_CUDA(cudaFuncSetAttribute(pass_kernel<B, kModeOdd, FE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
   RR_CUDA(cudaFuncSetAttribute(pass_kernel<B, kModeEven, FE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-  RR_CUDA(cudaFuncSetAttribute(pass_kernel<B, kModeGram, FE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
   return RR_OK;
 }
 
@@ -1394,14 +1305,16 @@ static int occupancy_B(rr_krylov* kr, int* pass_blocks, int* chunk_blocks, int* 
   const size_t sm = pass_smem_bytes<B>();
   if (kr->fold4) {
     RR_TRY((set_pass_smem<B, 4>()));
-    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(pass_blocks, pass_kernel<B, kModeGram, 4>, kThreads, sm));
+    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(pass_blocks, pass_kernel<B, kModeOdd, 4>, kThreads, sm));
     RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(chunk_blocks, chunk_kernel<B, 4>, kThreads, 0));
-    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(lean_blocks, lean_kernel<B, kModeOdd, 4>(), kThreads, 0));
+    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(lean_blocks, pass_kernel<B, kModeOdd, 4, false, kLeanLpt<B>>,
+                                                          kThreads, 0));
   } else {
     RR_TRY((set_pass_smem<B, 2>()));
-    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(pass_blocks, pass_kernel<B, kModeGram, 2>, kThreads, sm));
+    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(pass_blocks, pass_kernel<B, kModeOdd, 2>, kThreads, sm));
     RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(chunk_blocks, chunk_kernel<B, 2>, kThreads, 0));
-    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(lean_blocks, lean_kernel<B, kModeOdd, 2>(), kThreads, 0));
+    RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(lean_blocks, pass_kernel<B, kModeOdd, 2, false, kLeanLpt<B>>,
+                                                          kThreads, 0));
   }
   return RR_OK;
 }
@@ -1529,9 +1442,6 @@ int rows_per_batch(int B, int lpt) {
 }
 
 int krylov_occupancy(rr_krylov* kr) {
-  if (kr->B == 16)
-    RR_CUDA(cudaFuncSetAttribute(gram_tc_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)gram_tc_smem_bytes<16>()));
   if (kr->B == 32)
     RR_CUDA(cudaFuncSetAttribute(gram_tc_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)gram_tc_smem_bytes<32>()));
@@ -1612,9 +1522,15 @@ int krylov_launch_application(rr_krylov* kr, cudaEvent_t* ev) {
   P.X = reinterpret_cast<const uint4*>(x);
   P.Y = reinterpret_cast<uint4*>(kr->U.ptr);
   P.scale = kr->dr_m.ptr;
+  const bool fused = kr->B <= 16;  // kFusedGram: the passes add their own Gram terms
+  if (fused) {
+    P.gram_mul = kr->M.r1;  // the odd pass sums z R^{-1} (x) U
+    P.term_ctr = kr->d_term.ptr;
+    P.S_ptr = kr->d_sptr.ptr;
+  }
   RR_TRY(launch_pass(kr, P, kModeOdd));
   // odd term: sum over rows of z (x) U with z = U d_r^{-1}
-  {
+  if (!fused) {
     PassParams G = base_params(kr);
     G.rows = mat->A.rows;
     G.X = reinterpret_cast<const uint4*>(kr->U.ptr);
@@ -1636,9 +1552,10 @@ int krylov_launch_application(rr_krylov* kr, cudaEvent_t* ev) {
   P.Y = reinterpret_cast<uint4*>(xn);
   P.scale = kr->dc_m.ptr;
   P.scale2 = kr->dc_r.ptr;
+  P.gram_mul = 1;
   RR_TRY(launch_pass(kr, P, kModeEven));
   // even term: sum over rows of w' (x) w' with w' = x' d_c^{-1}
-  {
+  if (!fused) {
     PassParams G = base_params(kr);
     G.rows = mat->At.rows;
     G.X = reinterpret_cast<const uint4*>(xn);
