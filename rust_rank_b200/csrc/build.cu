@@ -218,12 +218,13 @@ int degree_order_device(const uint32_t* deg, int64_t n, uint32_t maxd, DevBuf<in
 // at most kChunkNnz entries, ordered (stably) by their first column, so that
 // chunks gathering the same region of the input block run together.  A row
 // whose chunks would each span more than one panel of kPanelCols columns of
-// the input block (rows of at least kChunkNnz entries per panel are dense
+// the input block (rows of at least kPanelDense entries per panel are dense
 // enough not to) is first cut at the panel boundaries, as long as its pieces
 // keep kMinPiece entries on average: the pieces of different rows that fall in
 // one panel then run together and gather from one L2-sized slice of the block.
 constexpr uint32_t kPanelCols = 1u << 18;
 constexpr int64_t kMinPiece = 64;
+constexpr int64_t kPanelDense = 1024;
 
 int build_chunks(DevCsr& d, int64_t heavy, cudaStream_t s) {
   d.heavy_rows = heavy;
@@ -253,7 +254,7 @@ int build_chunks(DevCsr& d, int64_t heavy, cudaStream_t s) {
   };
   for (int64_t r = 0; r < heavy; ++r) {
     const int64_t deg = (int64_t)ptr[r + 1] - ptr[r];
-    if (P > 1 && deg >= kMinPiece * P && deg < (int64_t)kChunkNnz * P) {
+    if (P > 1 && deg >= kMinPiece * P && deg < kPanelDense * P) {
       const uint32_t* pr = pos.data() + (size_t)r * (P + 1);
       for (int j = 0; j < P; ++j) cut(r, j == 0 ? ptr[r] : pr[j], j == P - 1 ? ptr[r + 1] : pr[j + 1]);
     } else {

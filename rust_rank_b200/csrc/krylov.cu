@@ -624,7 +624,7 @@ __global__ void __launch_bounds__(kThreads, (B >= 32 && GRAM ? 2 : 4)) pass_kern
 // 16-lane row in one warp load instruction, one L1 line look-up per gathered
 // row) at padded width 16, the pass kernels' default otherwise.
 template <int B>
-constexpr int kLeanLpt = (B >= 16) ? 4 : kDefaultLpt<B>;
+constexpr int kLeanLpt = (B == 16) ? 4 : kDefaultLpt<B>;
 
 // Padded widths whose single-matrix odd and even passes compute their Gram
 // terms themselves (u8-limb mma.sync on the block rows still in registers);
@@ -645,16 +645,14 @@ constexpr bool kFusedGram = (B <= 16);
 // in TMEM) computes all 16 limb pairs at once: A row (a, i) holds limb a of
 // lane i of the tile's rows (K = rows), B row (c, j) limb c of gu; M = 128
 // (4 B rows, zero-padded to 128 for B = 16), N = 4 B.  A CTA stages 128-row
-// tiles into double-buffered shared memory in the canonical K-major layout
-// without swizzle (8-row x 16-byte core matrices; K-adjacent cores 128 bytes
-// apart, 8-row groups 256 bytes apart), one thread issues the four K = 32
-// MMAs of a tile and commits them to the buffer's mbarrier.  A per-row limb
-// product is < 2^16, so the int32 accumulators are drained into registers
-// every kTcDrain tiles.  At the end the four warps read D out of TMEM
-// (tcgen05.ld), weight limb pairs by 2^{8(a+c)} mod p, and the CTA's sums join
-// the same replicated 64-bit accumulators and last-CTA finish as the pass
-// kernels.  Every wait on an mbarrier gives up after 2 s and sets *status.
-constexpr int kTcRows = 256;        // rows (K bytes) per tile
+// tiles into shared memory in the canonical K-major layout without swizzle
+// (8-row x 16-byte core matrices; K-adjacent cores 128 bytes apart, 8-row
+// groups 256 bytes apart); one thread issues the four K = 32 MMAs of a tile.
+// A per-row limb product is < 2^16, so the int32 accumulators are read out
+// every kTcDrain tiles (tcgen05.ld), limb pairs weighted by 2^{8(a+c)} mod p,
+// and the CTA's sums join the same replicated 64-bit accumulators and
+// last-CTA finish as the pass kernels.  Every wait on an mbarrier gives up
+// after 2 s and sets *status.
 constexpr int kTcDrain = 64;        // tiles between drains of the int32 accumulators
 constexpr uint64_t kTcWaitLimitNs = 2000000000ull;  // 2 s of %globaltimer
 
@@ -703,30 +701,54 @@ __device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity) {
   }
 }
 
-constexpr int kTcThreads = 512;  // Gram pass CTA: 16 warps, one CTA per SM
-
+// Warp roles of the Gram pass CTA (one CTA per SM):
+//   warp 0     producer: lane 0 keeps a ring of RING raw tiles filled by 1-D
+//              bulk copies (block rows and row scales of one tile each);
+//   warp 1     MMA issuer: lane 0 issues the tile's K = 32 UMMAs into one of
+//              two TMEM accumulators and commits them to the stage's mbarrier;
+//   warps 2-5  epilogue: every kTcDrain tiles they read the finished
+//              accumulator (tcgen05.ld; warp w owns TMEM lanes 32 (w % 4)),
+//              weight the limb pairs and free it, while the MMAs go on in the
+//              other accumulator;
+//   warps 6-   transposers, NG groups of TW warps, group g taking tiles
+//              j = g mod NG: scale the rows, split them into byte limbs and
+//              store them in operand stage j mod OPS.
+// Hand-offs are mbarriers only (no CTA-wide barrier inside the loop): raw
+// slot full (bulk-copy bytes) / empty (TW arrivals), operand stage full (TW
+// arrivals) / empty (MMA commit), accumulator full (commit) / empty (4
+// arrivals).  Every wait gives up after 2 s or once another role gave up.
 template <int B>
 struct TcShape {
-  static constexpr int MR = 4 * B;              // real A rows (limb, lane)
-  static constexpr int M = 128;                 // UMMA M (zero rows above MR)
-  static constexpr int N = 4 * B;               // UMMA N
-  static constexpr int A_BYTES = M * kTcRows;   // per operand buffer
-  static constexpr int B_BYTES = N * kTcRows;
-  static constexpr int OPS_BYTES = 2 * (A_BYTES + B_BYTES);  // two operand buffers
-  static constexpr int RAW_Y = kTcRows * B * 4;              // a tile's block rows
-  static constexpr int RAW_BYTES = RAW_Y + kTcRows * 4;      // plus its row scales
-  static constexpr int RING = B >= 32 ? 2 : 4;               // raw tiles in flight
-  static constexpr int COLS = N <= 64 ? 64 : 128;            // TMEM columns allocated
+  static constexpr int TILE = 128;                           // rows (K bytes) per tile
+  static constexpr int MR = 4 * B;                           // real A rows (limb, lane)
+  static constexpr int M = 128;                              // UMMA M (zero rows above MR)
+  static constexpr int N = 4 * B;                            // UMMA N
+  static constexpr int A_BYTES = M * TILE;
+  static constexpr int B_BYTES = N * TILE;
+  static constexpr int STAGE = A_BYTES + B_BYTES;            // one operand stage
+  static constexpr int OPS = 4;                              // operand stages
+  static constexpr int RAW_Y = TILE * B * 4;                 // a tile's block rows
+  static constexpr int RAW_BYTES = RAW_Y + TILE * 4;         // plus its row scales
+  static constexpr int RING = 4;                             // raw tiles in flight
+  static constexpr int GROUPS = B / 4;                       // 128-bit words per row
+  static constexpr int TASKS = (TILE / 4) * GROUPS;          // 4 rows x 4 lanes each
+  static constexpr int TW = TASKS / 32;                      // transposer warps per tile
+  static constexpr int NG = 2;                               // tiles transposed at once
+  static constexpr int XW0 = 6;                              // first transposer warp
+  static constexpr int WARPS = XW0 + NG * TW;
+  static constexpr int THREADS = 32 * WARPS;
+  static constexpr int COLS = 2 * N <= 128 ? 128 : 256;      // two accumulators
   static constexpr uint32_t IDESC = (2u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+  static_assert(TASKS % 32 == 0 && OPS % NG == 0 && RING % NG == 0, "tile shape");
 };
 
 template <int B>
 constexpr size_t gram_tc_smem_bytes() {
-  return (size_t)TcShape<B>::OPS_BYTES + (size_t)TcShape<B>::RING * TcShape<B>::RAW_BYTES;
+  return (size_t)TcShape<B>::OPS * TcShape<B>::STAGE + (size_t)TcShape<B>::RING * TcShape<B>::RAW_BYTES;
 }
-// dynamic + static (the CTA sums) within the 227 KB a CTA may hold
-static_assert(gram_tc_smem_bytes<16>() + 16 * 16 * 8 + 1024 <= 232448, "Gram tile ring too large");
-static_assert(gram_tc_smem_bytes<32>() + 32 * 32 * 8 + 1024 <= 232448, "Gram tile ring too large");
+// dynamic + static (the CTA sums, barriers) within the 227 KB a CTA may hold
+static_assert(gram_tc_smem_bytes<16>() + 16 * 16 * 8 + 1024 <= 232448, "Gram stages too large");
+static_assert(gram_tc_smem_bytes<32>() + 32 * 32 * 8 + 1024 <= 232448, "Gram stages too large");
 
 __device__ __forceinline__ void byte_transpose4(const uint32_t (&v)[4], uint32_t (&w)[4]) {
   // w[a] = bytes a of v[0..3]: limb a of four consecutive rows
@@ -738,14 +760,37 @@ __device__ __forceinline__ void byte_transpose4(const uint32_t (&v)[4], uint32_t
   w[3] = __byte_perm(t2, t3, 0x7632);
 }
 
-// Thread 0: the raw rows (and scales) of `tile` into ring slot `dst` by two
-// 1-D bulk copies completing on `mbar` (rows past the end are not copied; the
-// scale copy is rounded up to 16 bytes, which the scale arrays are padded for).
+// A bounded wait that also ends when another role of the CTA gave up.
+__device__ __forceinline__ bool mbar_wait_or(uint32_t addr, uint32_t parity, const volatile int* abort) {
+  const uint64_t t0 = tc_ns();
+  for (;;) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(done)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (*abort) return false;
+    if (tc_ns() - t0 > kTcWaitLimitNs) return false;
+  }
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Thread 0 of the producer: the raw rows (and scales) of `tile` into ring
+// slot `dst` by two 1-D bulk copies completing on `mbar` (rows past the end
+// are not copied; the scale copy is rounded up to 16 bytes, which the scale
+// arrays are padded for).
 template <int B>
 __device__ __forceinline__ void tc_fetch(const PassParams& P, int64_t tile, unsigned char* dst, uint64_t* mbar) {
   using T = TcShape<B>;
-  const int64_t r0 = tile * kTcRows;
-  const int rows = (int)(P.rows - r0 < kTcRows ? P.rows - r0 : kTcRows);
+  const int64_t r0 = tile * T::TILE;
+  const int rows = (int)(P.rows - r0 < T::TILE ? P.rows - r0 : T::TILE);
   const uint32_t ybytes = (uint32_t)rows * B * 4;
   const uint32_t sbytes = (uint32_t)((rows * 4 + 15) & ~15);
   const uint32_t mb = smem_u32(mbar);
@@ -761,31 +806,45 @@ __device__ __forceinline__ void tc_fetch(const PassParams& P, int64_t tile, unsi
 }
 
 template <int B>
-__global__ void __launch_bounds__(kTcThreads, 1) gram_tc_kernel(PassParams P, int* status) {
+__global__ void __launch_bounds__(TcShape<B>::THREADS, 1) gram_tc_kernel(PassParams P, int* status) {
   using T = TcShape<B>;
   constexpr int NP = B * (B + 1) / 2;
-  constexpr int GROUPS = B / 4;                       // 128-bit words per row
-  constexpr int TASKS = (kTcRows / 4) * GROUPS;       // 4 rows x 4 lanes each
   extern __shared__ __align__(1024) unsigned char tc_smem[];
-  __shared__ __align__(8) uint64_t mbar[2];           // MMA completion per operand buffer
-  __shared__ __align__(8) uint64_t rbar[T::RING];     // bulk-copy completion per raw slot
+  __shared__ __align__(8) uint64_t raw_full[T::RING], raw_empty[T::RING];
+  __shared__ __align__(8) uint64_t op_full[T::OPS], op_empty[T::OPS];
+  __shared__ __align__(8) uint64_t acc_full[2], acc_empty[2], fin;
   __shared__ uint32_t tmem_base_s;
   __shared__ unsigned long long red[B * B];
   __shared__ bool is_last;
-  __shared__ int s_fail;
-  unsigned char* const raw0 = tc_smem + T::OPS_BYTES;
+  __shared__ volatile int s_fail;
+  __shared__ int64_t s_issued;
+  unsigned char* const raw0 = tc_smem + T::OPS * T::STAGE;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const ModP M = P.M;
 
-  // zero the operand buffers once (the A rows above 4B stay zero), the CTA sums, the barriers
-  for (int e = tid; e < T::OPS_BYTES / 16; e += kTcThreads) reinterpret_cast<uint4*>(tc_smem)[e] = make_uint4(0, 0, 0, 0);
-  for (int e = tid; e < B * B; e += kTcThreads) red[e] = 0;
+  // zero the operand stages once (the A rows above 4B stay zero), the CTA sums, the barriers
+  for (int e = tid; e < T::OPS * T::STAGE / 16; e += T::THREADS)
+    reinterpret_cast<uint4*>(tc_smem)[e] = make_uint4(0, 0, 0, 0);
+  for (int e = tid; e < B * B; e += T::THREADS) red[e] = 0;
   if (tid == 0) {
     s_fail = 0;
-    for (int i = 0; i < 2; ++i)
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[i])) : "memory");
-    for (int i = 0; i < T::RING; ++i)
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&rbar[i])) : "memory");
+    s_issued = 0;
+    auto init = [](uint64_t* bar, int count) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+    };
+    for (int i = 0; i < T::RING; ++i) {
+      init(&raw_full[i], 1);
+      init(&raw_empty[i], T::TW);
+    }
+    for (int i = 0; i < T::OPS; ++i) {
+      init(&op_full[i], T::TW);
+      init(&op_empty[i], 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      init(&acc_full[i], 1);
+      init(&acc_empty[i], 4);
+    }
+    init(&fin, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
@@ -794,53 +853,105 @@ __global__ void __launch_bounds__(kTcThreads, 1) gram_tc_kernel(PassParams P, in
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the zeroed stages, for the tensor cores
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_base_s;
 
-  const int64_t ntiles = (P.rows + kTcRows - 1) / kTcRows;
+  const int64_t ntiles = (P.rows + T::TILE - 1) / T::TILE;
   const int64_t mine = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;  // tiles of this CTA
-  if (tid == 0) {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    for (int64_t j = 0; j < mine && j < T::RING; ++j)
-      tc_fetch<B>(P, blockIdx.x + j * gridDim.x, raw0 + j * T::RAW_BYTES, &rbar[j]);
-  }
+  auto give_up = [&]() {
+    s_fail = 1;
+    atomicExch(status, 1);
+  };
 
-  // per-thread sums of the drained limb products: thread (warp w < 4, lane l)
-  // owns A row m = 32 w + l = (a, i) (tc_row) and keeps
-  // sum_c 256^{a+c} D[m][(c, j)] mod p per j
+  // epilogue state: thread (warp w in 2..5, lane l) owns A row m = 32 (w % 4)
+  // + l = (a, i) and keeps sum_c 256^{a+c} D[m][(c, j)] mod p per lane j
   uint32_t part[B];
 #pragma unroll
   for (int j = 0; j < B; ++j) part[j] = 0;
-  const int m_row = 32 * warp + lane;
-  const bool reader = warp < 4 && m_row < T::MR;
-  const int a_limb = m_row / B;
-  uint32_t wgt[4];  // 2^{8(a + c)} mod p for c = 0..3
-  {
-    uint64_t w = 1;
-    for (int e = 0; e < (reader ? a_limb : 0); ++e) w = w * 256 % M.p;
-    for (int c = 0; c < 4; ++c) {
-      wgt[c] = (uint32_t)w;
-      w = w * 256 % M.p;
-    }
-  }
-  uint32_t commits[2] = {0, 0};
-  auto drain = [&]() {
-    if (tid == 0) {
-      for (int q = 0; q < 2; ++q)
-        if (commits[q] && !mbar_wait(smem_u32(&mbar[q]), (commits[q] - 1) & 1)) {
-          s_fail = 1;
-          atomicExch(status, 1);
+  const int quad = warp & 3;
+  const int m_row = 32 * quad + lane;
+  const bool reader = warp >= 2 && warp < 6 && m_row < T::MR;
+
+  if (warp == 0) {
+    // ------------------------------------------------------------ producer
+    if (lane == 0) {
+      for (int64_t j = 0; j < mine; ++j) {
+        const int slot = (int)(j % T::RING);
+        if (j >= T::RING && !mbar_wait_or(smem_u32(&raw_empty[slot]), (uint32_t)((j / T::RING - 1) & 1), &s_fail)) {
+          give_up();
+          break;
         }
+        tc_fetch<B>(P, blockIdx.x + j * gridDim.x, raw0 + slot * T::RAW_BYTES, &raw_full[slot]);
+        s_issued = j + 1;
+      }
     }
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (warp < 4) {
+  } else if (warp == 1) {
+    // ------------------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      for (int64_t j = 0; j < mine; ++j) {
+        const int s = (int)(j % T::OPS);
+        const int64_t grp = j / kTcDrain;
+        const int a = (int)(grp & 1);
+        const bool first = j % kTcDrain == 0;
+        if (first && grp >= 2 && !mbar_wait_or(smem_u32(&acc_empty[a]), (uint32_t)((grp / 2 - 1) & 1), &s_fail)) {
+          give_up();
+          break;
+        }
+        if (!mbar_wait_or(smem_u32(&op_full[s]), (uint32_t)((j / T::OPS) & 1), &s_fail)) {
+          give_up();
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t a0 = smem_u32(tc_smem + s * T::STAGE), b0 = a0 + T::A_BYTES;
+#pragma unroll
+        for (int kb = 0; kb < T::TILE / 32; ++kb) {
+          const uint64_t da = umma_desc(a0 + kb * (T::M / 8) * 256);
+          const uint64_t db = umma_desc(b0 + kb * (T::N / 8) * 256);
+          const uint32_t accum = (!first || kb > 0) ? 1u : 0u;
+          asm volatile(
+              "{\n\t.reg .pred p;\n\t"
+              "setp.ne.b32 p, %4, 0;\n\t"
+              "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+              :
+              : "r"(tmem + (uint32_t)(a * T::N)), "l"(da), "l"(db), "r"(T::IDESC), "r"(accum), "r"(0u), "r"(0u),
+                "r"(0u), "r"(0u)
+              : "memory");
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_u32(&op_empty[s]))
+                     : "memory");
+        if (j % kTcDrain == kTcDrain - 1 || j == mine - 1)
+          asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                           smem_u32(&acc_full[a]))
+                       : "memory");
+      }
+    }
+  } else if (warp < T::XW0) {
+    // ------------------------------------------------------------ epilogue
+    uint32_t wgt[4];  // 2^{8(a + c)} mod p for c = 0..3, a = this row's limb
+    {
+      uint64_t w = 1;
+      for (int e = 0; e < (reader ? m_row / B : 0); ++e) w = w * 256 % M.p;
+      for (int c = 0; c < 4; ++c) {
+        wgt[c] = (uint32_t)w;
+        w = w * 256 % M.p;
+      }
+    }
+    const int64_t ngrp = (mine + kTcDrain - 1) / kTcDrain;
+    for (int64_t G = 0; G < ngrp; ++G) {
+      const int a = (int)(G & 1);
+      if (!mbar_wait_or(smem_u32(&acc_full[a]), (uint32_t)((G / 2) & 1), &s_fail)) {
+        give_up();
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
       for (int c0 = 0; c0 < T::N; c0 += 16) {
         uint32_t v[16];
-        const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0;
+        const uint32_t taddr = tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)(a * T::N + c0);
         asm volatile(
             "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
             : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
@@ -856,48 +967,41 @@ __global__ void __launch_bounds__(kTcThreads, 1) gram_tc_kernel(PassParams P, in
           }
         }
       }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acc_empty[a]);
     }
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
-  };
-
-  bool acc_live = false;  // D holds sums to accumulate onto
-  int64_t jstop = mine;   // the tile at which a wait gave up
-  for (int64_t j = 0; j < mine; ++j) {
-    const int slot = (int)(j % T::RING), s = (int)(j & 1);
-    unsigned char* const raw = raw0 + slot * T::RAW_BYTES;
-    unsigned char* const bufA = tc_smem + s * (T::A_BYTES + T::B_BYTES);
-    unsigned char* const bufB = bufA + T::A_BYTES;
-    // the raw tile has landed (every thread polls the barrier) and the MMAs
-    // of tile j - 2 no longer read operand buffer s
-    if (!mbar_wait(smem_u32(&rbar[slot]), (uint32_t)((j / T::RING) & 1))) {
-      s_fail = 1;
-      atomicExch(status, 1);
-    }
-    if (j >= 2 && tid == 0 && !mbar_wait(smem_u32(&mbar[s]), (commits[s] - 1) & 1)) {
-      s_fail = 1;
-      atomicExch(status, 1);
-    }
-    __syncthreads();
-    if (s_fail) {
-      jstop = j;
-      break;
-    }
-    const int64_t r0 = (blockIdx.x + j * gridDim.x) * kTcRows;
-    const uint32_t* scl = reinterpret_cast<const uint32_t*>(raw + T::RAW_Y);
-    for (int task = tid; task < TASKS; task += kTcThreads) {
-      const int g = task % GROUPS, qd = task / GROUPS;
+  } else {
+    // ------------------------------------------------------------ transposers
+    const int xw = warp - T::XW0, g = xw / T::TW;
+    const int task = (xw % T::TW) * 32 + lane;
+    const int gw = task % T::GROUPS, qd = task / T::GROUPS;  // word gw of rows 4 qd .. 4 qd + 3
+    for (int64_t j = g; j < mine; j += T::NG) {
+      const int slot = (int)(j % T::RING), s = (int)(j % T::OPS);
+      if (!mbar_wait_or(smem_u32(&raw_full[slot]), (uint32_t)((j / T::RING) & 1), &s_fail)) {
+        give_up();
+        break;
+      }
+      if (j >= T::OPS && !mbar_wait_or(smem_u32(&op_empty[s]), (uint32_t)((j / T::OPS - 1) & 1), &s_fail)) {
+        give_up();
+        break;
+      }
+      const unsigned char* raw = raw0 + slot * T::RAW_BYTES;
+      const uint32_t* scl = reinterpret_cast<const uint32_t*>(raw + T::RAW_Y);
+      unsigned char* const bufA = tc_smem + s * T::STAGE;
+      unsigned char* const bufB = bufA + T::A_BYTES;
+      const int64_t r0 = (blockIdx.x + j * gridDim.x) * T::TILE;
       uint4 y[4];
       uint32_t sc[4];
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         const int rr = 4 * qd + q;
         const bool in = r0 + rr < P.rows;
-        y[q] = in ? *reinterpret_cast<const uint4*>(raw + ((size_t)rr * B + 4 * g) * 4) : make_uint4(0, 0, 0, 0);
+        y[q] = in ? *reinterpret_cast<const uint4*>(raw + ((size_t)rr * B + 4 * gw) * 4) : make_uint4(0, 0, 0, 0);
         sc[q] = in ? scl[rr] : 0u;
       }
 #pragma unroll
-      for (int c4 = 0; c4 < 4; ++c4) {  // lane 4 g + c4
+      for (int c4 = 0; c4 < 4; ++c4) {  // lane 4 gw + c4
         uint32_t z[4], u[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
@@ -910,53 +1014,34 @@ __global__ void __launch_bounds__(kTcThreads, 1) gram_tc_kernel(PassParams P, in
         byte_transpose4(u, wu);
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
-          *reinterpret_cast<uint32_t*>(bufA + tc_off(T::M, a * B + c4 * GROUPS + g, 4 * qd)) = wz[a];
-          *reinterpret_cast<uint32_t*>(bufB + tc_off(T::N, a * B + c4 * GROUPS + g, 4 * qd)) = wu[a];
+          *reinterpret_cast<uint32_t*>(bufA + tc_off(T::M, a * B + c4 * T::GROUPS + gw, 4 * qd)) = wz[a];
+          *reinterpret_cast<uint32_t*>(bufB + tc_off(T::N, a * B + c4 * T::GROUPS + gw, 4 * qd)) = wu[a];
         }
       }
-    }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();  // operand buffer s written, raw slot read by every thread
-    if (tid == 0) {
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t a0 = smem_u32(bufA), b0 = smem_u32(bufB);
-#pragma unroll
-      for (int kb = 0; kb < kTcRows / 32; ++kb) {
-        const uint64_t da = umma_desc(a0 + kb * (T::M / 8) * 256);
-        const uint64_t db = umma_desc(b0 + kb * (T::N / 8) * 256);
-        const uint32_t accum = (acc_live || kb > 0) ? 1u : 0u;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "setp.ne.b32 p, %4, 0;\n\t"
-            "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
-            :
-            : "r"(tmem), "l"(da), "l"(db), "r"(T::IDESC), "r"(accum), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
-            : "memory");
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // stores visible to the tensor cores
+      __syncwarp();
+      if (lane == 0) {
+        mbar_arrive(&op_full[s]);
+        mbar_arrive(&raw_empty[slot]);
       }
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                       smem_u32(&mbar[s]))
-                   : "memory");
-      // refill the raw slot just read with the tile RING ahead
-      if (j + T::RING < mine) tc_fetch<B>(P, blockIdx.x + (j + T::RING) * gridDim.x, raw, &rbar[slot]);
-    }
-    commits[s] += 1;
-    acc_live = true;
-    if ((j + 1) % kTcDrain == 0) {
-      drain();
-      acc_live = false;
     }
   }
-  if (acc_live && !s_fail) drain();
+  __syncthreads();
   if (s_fail) {  // let what was committed or fetched finish before the memory goes away
-    if (tid == 0) {
-      for (int q = 0; q < 2; ++q)
-        if (commits[q]) mbar_wait(smem_u32(&mbar[q]), (commits[q] - 1) & 1);
-      // fetches still unconsumed: tiles [jstop, min(mine, jstop + RING)), one per slot
-      for (int64_t j = jstop; j < mine && j < jstop + T::RING; ++j)
-        mbar_wait(smem_u32(&rbar[(int)(j % T::RING)]), (uint32_t)((j / T::RING) & 1));
+    if (tid == 32) {
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_u32(&fin))
+                   : "memory");
+      mbar_wait(smem_u32(&fin), 0);
     }
-    __syncthreads();
+    if (tid == 0) {  // the last RING fetches issued, one per slot
+      const int64_t hi = s_issued;
+      for (int64_t j = hi > T::RING ? hi - T::RING : 0; j < hi; ++j)
+        mbar_wait(smem_u32(&raw_full[(int)(j % T::RING)]), (uint32_t)((j / T::RING) & 1));
+    }
   }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
   if (warp == 0) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(T::COLS) : "memory");
@@ -969,7 +1054,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) gram_tc_kernel(PassParams P, in
   }
   __syncthreads();
   unsigned long long* const acc = P.gram_acc + (size_t)(blockIdx.x % P.replicas) * P.gram_stride;
-  for (int q = tid; q < NP; q += kTcThreads) {
+  for (int q = tid; q < NP; q += T::THREADS) {
     int i, jj;
     pair_of(q, B, i, jj);
     atomicAdd(&acc[q], (unsigned long long)reduce(red[i * B + jj], M));
@@ -984,7 +1069,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) gram_tc_kernel(PassParams P, in
   const int b = P.b_real;
   const int npr = b * (b + 1) / 2;
   uint32_t* S_out = *P.S_ptr + (size_t)__ldcg(P.term_ctr) * npr;
-  for (int q = tid; q < npr; q += kTcThreads) {
+  for (int q = tid; q < npr; q += T::THREADS) {
     int i, jj;
     pair_of(q, b, i, jj);
     const int qb = pair_index(i, jj, B);
@@ -993,7 +1078,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) gram_tc_kernel(PassParams P, in
     S_out[q] = mulmod(reduce(v, M), P.gram_mul, M);
   }
   __syncthreads();
-  for (int q = tid; q < NP * P.replicas; q += kTcThreads)
+  for (int q = tid; q < NP * P.replicas; q += T::THREADS)
     __stcg(P.gram_acc + (size_t)(q / NP) * P.gram_stride + q % NP, 0ull);
   if (tid == 0) {
     *P.term_ctr += 1u;
@@ -1079,17 +1164,14 @@ __global__ void barrier_check_kernel(unsigned int* bar, int* error, uint64_t lim
     if (!grid_barrier(bar, error, limit_ns, expected)) return;
 }
 
-// Long rows: one warp per chunk of at most kChunkNnz entries.  Lanes form RPW
-// slots of TPR threads; slot s takes entries beg+s, beg+s+RPW, ...  The slot
-// sums (exact residues) are combined with shuffles and added to heavy_acc with
-// 64-bit atomics.  L = 4 lanes per thread at widths 16 and 32: each gathered
-// row is read whole by one warp load instruction (64 or 128 bytes), so the
-// L1 data pipe handles half as many wavefronts per gathered byte as with rows
-// split over two instructions.
-template <int B>
-constexpr int kChunkLpt = (B >= 16) ? 4 : kDefaultLpt<B>;
-
-template <int B, int FE, int L = kChunkLpt<B>>
+// Long rows: one warp per chunk of at most kChunkNnz entries, warps taking the
+// next chunk from a dispenser (an atomic ticket), so that the kernel ends
+// within about one chunk's time of its last warp.  Lanes form RPW slots of TPR
+// threads; slot s takes entries beg+s, beg+s+RPW, ...  The slot sums (exact
+// residues) are combined with shuffles and added to heavy_acc with 64-bit
+// atomics.  (4 lanes per thread at widths 16 and 32, a whole gathered row per
+// load instruction, measured slower: fewer bytes in flight per thread.)
+template <int B, int FE, int L = kDefaultLpt<B>>
 __global__ void __launch_bounds__(kThreads, 3) chunk_kernel(ChunkParams P) {
   using S = Shape<B, L>;
   constexpr int LPT = S::LPT, TPR = S::TPR, RPW = S::RPW;
@@ -1097,9 +1179,11 @@ __global__ void __launch_bounds__(kThreads, 3) chunk_kernel(ChunkParams P) {
   const int sub = lane % TPR;
   const int slot = lane / TPR;
   const ModP M = P.M;
-  const int64_t gw = (int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5);
-  const int64_t nw = (int64_t)gridDim.x * kWarps;
-  for (int64_t ch = gw; ch < P.nchunks; ch += nw) {
+  for (;;) {
+    unsigned int ticket = 0;
+    if (lane == 0) ticket = atomicAdd(P.next, 1u);
+    const int64_t ch = __shfl_sync(0xffffffffu, ticket, 0);
+    if (ch >= P.nchunks) break;
     const uint32_t beg = P.chunk_begin[ch], end = P.chunk_end[ch];
     const uint32_t row = P.chunk_row[ch];
     uint64_t acc[LPT];
@@ -1240,9 +1324,9 @@ static int launch_pass_BF(rr_krylov* kr, const PassParams& P, int mode, dim3 gri
 // Gram passes at padded width 32 run on tcgen05 (gram_tc_kernel).
 template <int B>
 static int launch_gram_tc(rr_krylov* kr, const PassParams& P, cudaStream_t s) {
-  const int64_t ntiles = (P.rows + kTcRows - 1) / kTcRows;
+  const int64_t ntiles = (P.rows + TcShape<B>::TILE - 1) / TcShape<B>::TILE;
   const dim3 grid((unsigned)std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)kr->mat->ctx->num_sms)));
-  return launch_ex(kr, gram_tc_kernel<B>, grid, dim3(kTcThreads), gram_tc_smem_bytes<B>(), s, P,
+  return launch_ex(kr, gram_tc_kernel<B>, grid, dim3(TcShape<B>::THREADS), gram_tc_smem_bytes<B>(), s, P,
                         kr->d_status.ptr);
 }
 
@@ -1500,7 +1584,10 @@ static int run_chunks(rr_krylov* kr, const DevCsr& A, const uint32_t* X) {
   C.nchunks = A.nchunks;
   C.X = reinterpret_cast<const uint4*>(X);
   C.heavy_acc = kr->heavy_acc.ptr;
+  C.next = kr->chunk_next.ptr;
   C.M = kr->M;
+  cudaStream_t s = kr->launch_stream ? kr->launch_stream : kr->mat->ctx->stream;
+  RR_CUDA(cudaMemsetAsync(kr->chunk_next.ptr, 0, sizeof(unsigned int), s));
   return launch_chunk(kr, C);
 }
 

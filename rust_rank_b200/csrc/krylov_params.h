@@ -62,6 +62,7 @@ struct ChunkParams {
   int64_t nchunks;
   const uint4* X;
   unsigned long long* heavy_acc;
+  unsigned int* next;  // chunk dispenser: zero at launch, one ticket per warp fetch
   ModP M;
 };
 

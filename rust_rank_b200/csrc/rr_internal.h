@@ -144,7 +144,7 @@ struct DevCsr {
 };
 
 constexpr int64_t kHeavyDegree = 32;   // rows longer than this are split
-constexpr int64_t kChunkNnz = 1024;    // nonzeros per chunk of a split row
+constexpr int64_t kChunkNnz = 256;     // nonzeros per chunk of a split row
 
 }  // namespace rr
 
@@ -184,6 +184,7 @@ struct rr_krylov_s {
   int64_t launches = 0;  // kernels launched by this handle
   // device-indexed sequence output: next slot (len - base) and the S pointer
   rr::DevBuf<unsigned int> d_term;
+  rr::DevBuf<unsigned int> chunk_next;  // chunk_kernel dispenser
   rr::DevBuf<uint32_t*> d_sptr;
   // a captured run of kGraphApps applications, replayable when cur == graph_cur
   cudaGraphExec_t graph = nullptr;
