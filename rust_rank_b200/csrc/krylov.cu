@@ -626,14 +626,17 @@ __global__ void __launch_bounds__(kThreads, (B >= 32 && GRAM ? 2 : 4)) pass_kern
 template <int B>
 constexpr int kLeanLpt = (B == 16) ? 4 : kDefaultLpt<B>;
 
-// Padded widths whose single-matrix odd and even passes compute their Gram
-// terms themselves (u8-limb mma.sync on the block rows still in registers);
-// at width 32 the passes run without Gram terms and a tcgen05 Gram pass
-// (gram_tc_kernel) reads each written block once more.  Measured on the 2M x
-// 1.5M Zipf matrix: fused 0.63 ms per application at width 16 against 0.69
-// split; split 1.11 ms at width 32 against 1.29 fused.
+// Which single-matrix passes compute their Gram terms themselves (u8-limb
+// mma.sync on the block rows still in registers) and which run without them,
+// followed by a tcgen05 Gram pass (gram_tc_kernel) that reads the written
+// block once more.  Measured per pass on the 2M x 1.5M Zipf matrix: at width
+// 16 the odd pass is faster split (0.251 ms against 0.269 fused), the even
+// pass fused (0.146 against 0.173); at width 32 both are faster split (0.93
+// ms per application against 1.29 fused).
 template <int B>
-constexpr bool kFusedGram = (B <= 16);
+constexpr bool kFusedOdd = (B <= 8);
+template <int B>
+constexpr bool kFusedEven = (B <= 16);
 
 // ---------------------------------------------------------------- Gram pass on tcgen05
 // The Gram term of a block (kModeGram: gz = x * scale, gu = gram_sym ? gz : x
@@ -733,7 +736,7 @@ struct TcShape {
   static constexpr int GROUPS = B / 4;                       // 128-bit words per row
   static constexpr int TASKS = (TILE / 4) * GROUPS;          // 4 rows x 4 lanes each
   static constexpr int TW = TASKS / 32;                      // transposer warps per tile
-  static constexpr int NG = 2;                               // tiles transposed at once
+  static constexpr int NG = B >= 32 ? 2 : 4;                 // tiles transposed at once
   static constexpr int XW0 = 6;                              // first transposer warp
   static constexpr int WARPS = XW0 + NG * TW;
   static constexpr int THREADS = 32 * WARPS;
@@ -1300,11 +1303,11 @@ static int launch_ex(const rr_krylov* kr, void (*fn)(Args...), dim3 grid, dim3 b
   return RR_OK;
 }
 
-// Single-matrix launches: at widths up to 16 the odd and even passes add their
-// Gram terms themselves; at width 32 they run without them (no staging, no
-// tensor-core flush, so fewer registers and no shared memory), each followed
-// by a tcgen05 Gram pass over the block it wrote (kModeGram).  The initial
-// pass computes S_0 itself.
+// Single-matrix launches: a fused pass (kFusedOdd / kFusedEven) adds its Gram
+// term itself; a lean pass runs without it (no staging, no tensor-core flush,
+// so fewer registers and no shared memory) and is followed by a tcgen05 Gram
+// pass over the block it wrote (kModeGram).  The initial pass computes S_0
+// itself.
 template <int B, int FE>
 static int launch_pass_BF(rr_krylov* kr, const PassParams& P, int mode, dim3 grid, cudaStream_t s) {
   const dim3 block(kThreads);
@@ -1312,16 +1315,16 @@ static int launch_pass_BF(rr_krylov* kr, const PassParams& P, int mode, dim3 gri
   switch (mode) {
     case kModeInit: return launch_ex(kr, pass_kernel<B, kModeInit, FE, true>, grid, block, sm, s, P);
     case kModeOdd:
-      if constexpr (kFusedGram<B>) return launch_ex(kr, pass_kernel<B, kModeOdd, FE, true>, grid, block, sm, s, P);
+      if constexpr (kFusedOdd<B>) return launch_ex(kr, pass_kernel<B, kModeOdd, FE, true>, grid, block, sm, s, P);
       else return launch_ex(kr, pass_kernel<B, kModeOdd, FE, false, kLeanLpt<B>>, grid, block, 0, s, P);
     case kModeEven:
-      if constexpr (kFusedGram<B>) return launch_ex(kr, pass_kernel<B, kModeEven, FE, true>, grid, block, sm, s, P);
+      if constexpr (kFusedEven<B>) return launch_ex(kr, pass_kernel<B, kModeEven, FE, true>, grid, block, sm, s, P);
       else return launch_ex(kr, pass_kernel<B, kModeEven, FE, false, kLeanLpt<B>>, grid, block, 0, s, P);
   }
   return fail(RR_EINVAL, "pass mode %d has no pass kernel at width %d", mode, B);
 }
 
-// Gram passes at padded width 32 run on tcgen05 (gram_tc_kernel).
+// Gram passes (widths 16 and 32) run on tcgen05 (gram_tc_kernel).
 template <int B>
 static int launch_gram_tc(rr_krylov* kr, const PassParams& P, cudaStream_t s) {
   const int64_t ntiles = (P.rows + TcShape<B>::TILE - 1) / TcShape<B>::TILE;
@@ -1332,13 +1335,13 @@ static int launch_gram_tc(rr_krylov* kr, const PassParams& P, cudaStream_t s) {
 
 template <int B>
 static int launch_pass_B(rr_krylov* kr, const PassParams& P, int mode) {
-  if constexpr (B == 32) {
+  if constexpr (B >= 16) {
     if (mode == kModeGram) {
       cudaStream_t s = kr->launch_stream ? kr->launch_stream : kr->mat->ctx->stream;
-      return launch_gram_tc<32>(kr, P, s);
+      return launch_gram_tc<B>(kr, P, s);
     }
   }
-  const bool lean = !kFusedGram<B> && (mode == kModeOdd || mode == kModeEven);
+  const bool lean = (mode == kModeOdd && !kFusedOdd<B>) || (mode == kModeEven && !kFusedEven<B>);
   const dim3 grid(lean ? pass_grid_lean<B>(kr, P.rows) : pass_grid<B>(kr, P.rows));
   cudaStream_t s = kr->launch_stream ? kr->launch_stream : kr->mat->ctx->stream;
   return kr->fold4 ? launch_pass_BF<B, 4>(kr, P, mode, grid, s) : launch_pass_BF<B, 2>(kr, P, mode, grid, s);
@@ -1526,6 +1529,9 @@ int rows_per_batch(int B, int lpt) {
 }
 
 int krylov_occupancy(rr_krylov* kr) {
+  if (kr->B == 16)
+    RR_CUDA(cudaFuncSetAttribute(gram_tc_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)gram_tc_smem_bytes<16>()));
   if (kr->B == 32)
     RR_CUDA(cudaFuncSetAttribute(gram_tc_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)gram_tc_smem_bytes<32>()));
@@ -1609,15 +1615,16 @@ int krylov_launch_application(rr_krylov* kr, cudaEvent_t* ev) {
   P.X = reinterpret_cast<const uint4*>(x);
   P.Y = reinterpret_cast<uint4*>(kr->U.ptr);
   P.scale = kr->dr_m.ptr;
-  const bool fused = kr->B <= 16;  // kFusedGram: the passes add their own Gram terms
-  if (fused) {
+  // kFusedOdd / kFusedEven: passes that add their own Gram terms
+  const bool fused_odd = kr->B <= 8, fused_even = kr->B <= 16;
+  if (fused_odd) {
     P.gram_mul = kr->M.r1;  // the odd pass sums z R^{-1} (x) U
     P.term_ctr = kr->d_term.ptr;
     P.S_ptr = kr->d_sptr.ptr;
   }
   RR_TRY(launch_pass(kr, P, kModeOdd));
   // odd term: sum over rows of z (x) U with z = U d_r^{-1}
-  if (!fused) {
+  if (!fused_odd) {
     PassParams G = base_params(kr);
     G.rows = mat->A.rows;
     G.X = reinterpret_cast<const uint4*>(kr->U.ptr);
@@ -1640,9 +1647,13 @@ int krylov_launch_application(rr_krylov* kr, cudaEvent_t* ev) {
   P.scale = kr->dc_m.ptr;
   P.scale2 = kr->dc_r.ptr;
   P.gram_mul = 1;
+  if (fused_even) {
+    P.term_ctr = kr->d_term.ptr;
+    P.S_ptr = kr->d_sptr.ptr;
+  }
   RR_TRY(launch_pass(kr, P, kModeEven));
   // even term: sum over rows of w' (x) w' with w' = x' d_c^{-1}
-  if (!fused) {
+  if (!fused_even) {
     PassParams G = base_params(kr);
     G.rows = mat->At.rows;
     G.X = reinterpret_cast<const uint4*>(xn);

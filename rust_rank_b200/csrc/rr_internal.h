@@ -144,7 +144,7 @@ struct DevCsr {
 };
 
 constexpr int64_t kHeavyDegree = 32;   // rows longer than this are split
-constexpr int64_t kChunkNnz = 256;     // nonzeros per chunk of a split row
+constexpr int64_t kChunkNnz = 1024;    // nonzeros per chunk of a split row
 
 }  // namespace rr
 

@@ -68,3 +68,45 @@ def test_rejects_sizes_beyond_the_limit():
     with pytest.raises(rr.RRError) as e:
         noalloc_pm_basis(seq, 2, 33, P)
     assert e.value.status == 1 and "limit" in str(e.value)
+
+
+def test_captured_in_a_cuda_graph():
+    """The stated use inside stream capture: one call before capture (it looks
+    up the scratch array and sets the kernel attribute), one call captured
+    into a CUDA graph on a side stream, the graph replayed on new sequences:
+    each replay equals the regular entry point."""
+    import torch
+
+    b, d, p = 8, 32, P
+    np_, nlen = b * (b + 1) // 2, d + 1
+    rng = np.random.default_rng(77)
+    d_seq = torch.zeros((np_, nlen), dtype=torch.int32, device="cuda")
+    d_M = torch.zeros((2 * b, 2 * b, d + 1), dtype=torch.int32, device="cuda")
+    d_delta = torch.zeros((2 * b,), dtype=torch.int64, device="cuda")
+
+    def call(stream):
+        _lib.check(_lib.lib().rr_pm_basis_short_noalloc(C.c_void_p(d_seq.data_ptr()), nlen, b, nlen, d, p,
+                                                          C.c_void_p(d_M.data_ptr()), C.c_void_p(d_delta.data_ptr()),
+                                                          C.c_void_p(stream.cuda_stream)))
+
+    side = torch.cuda.Stream()
+    d_seq.copy_(torch.from_numpy(rng.integers(0, p, size=(np_, nlen)).astype(np.uint32).view(np.int32)))
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        call(side)  # first call: outside capture
+    side.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=side):
+        call(torch.cuda.current_stream())
+    for rep in range(2):
+        seq = rng.integers(0, p, size=(np_, nlen)).astype(np.uint32)
+        d_seq.copy_(torch.from_numpy(seq.view(np.int32)))
+        torch.cuda.synchronize()
+        graph.replay()
+        torch.cuda.synchronize()
+        M = d_M.cpu().numpy().view(np.uint32)
+        delta = d_delta.cpu().numpy()
+        M_ref, delta_ref = rr.PM_Basis(seq, d, p)
+        assert np.array_equal(M, M_ref), f"replay {rep}"
+        assert np.array_equal(delta, delta_ref), f"replay {rep}"
+    del graph
