@@ -376,8 +376,10 @@ def served_stream(nreq=12, rmin=10_000, rmax=2_000_000, rate=50.0, b=16, seed=48
 def full_rank_zipf(ctx, rowptr, col, val, m, n, b=16):
     """Host CSR in, rank out on the large Zipf matrix: rr_matrix_create (device
     build), the Krylov sequence of the stated length N/b + N/b + 32 (N = the
-    smaller dimension), the PM-basis of order d = largest power of two <= length,
-    and the rank readout -- all through the public API, timed by wall clock."""
+    smaller dimension) -- which the rank path, like src/main.rs:500-503, rounds
+    up to the next power of two for b > 1 -- the PM-basis of order d = largest
+    power of two <= length, and the rank readout, all through the public API,
+    timed by wall clock."""
     import rust_rank_b200 as rr
     from rust_rank_b200 import synth
 
@@ -391,7 +393,9 @@ def full_rank_zipf(ctx, rowptr, col, val, m, n, b=16):
     t2 = time.perf_counter()
     dm.close()
     nonempty = int(np.count_nonzero(np.bincount(col, minlength=n)))
-    return {"workload": f"zipf_{m}x{n}_nnz{int(rowptr[-1])}_b{b}", "sequence_terms": L + 1, "rank": rank,
+    L2 = 1 << (L - 1).bit_length() if b > 1 else L  # src/main.rs:500-503
+    return {"workload": f"zipf_{m}x{n}_nnz{int(rowptr[-1])}_b{b}", "stated_length": L, "sequence_terms": L2 + 1,
+            "applications_of_B": L2 // 2, "generator_order": L2, "rank": rank,
             "upper_bound_nonempty_columns": nonempty, "s_total": t2 - t0, "s_matrix_build": t1 - t0,
             "ranks_per_sec": 1.0 / (t2 - t0),
             "timing": "wall clock, host CSR in (pageable numpy arrays), rank out"}
