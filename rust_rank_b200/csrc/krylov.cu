@@ -163,6 +163,72 @@ __device__ __forceinline__ void gather_sum(const uint2* __restrict__ cv, uint32_
   }
 }
 
+// The same sum with eight entries per step (two groups of four in flight per
+// thread): with 4 lanes per thread a whole 64- or 128-byte block row is one
+// warp load instruction (one L1 wavefront per gathered row instead of two),
+// and the eight loads keep as many bytes in flight as four steps of 8 lanes.
+template <int B, int FE, int L>
+__device__ __forceinline__ void gather_sum8(const uint2* __restrict__ cv, uint32_t beg, uint32_t end, uint32_t stride,
+                                            const uint4* __restrict__ X, int sub, const ModP& M,
+                                            uint64_t (&acc)[Shape<B, L>::LPT]) {
+  constexpr int NV = Shape<B, L>::NV, TPR = Shape<B, L>::TPR;
+  constexpr int RW = B / 4;
+  const uint4* Xs = X + sub;
+  uint32_t k = beg;
+  if (k + 7 * stride < end) {
+    uint2 e0[4], e1[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      e0[u] = __ldg(cv + k + u * stride);
+      e1[u] = __ldg(cv + k + (u + 4) * stride);
+    }
+    for (;;) {
+      uint4 g0[4][NV], g1[4][NV];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          g0[u][v] = __ldg(Xs + (size_t)e0[u].x * RW + v * TPR);
+          g1[u][v] = __ldg(Xs + (size_t)e1[u].x * RW + v * TPR);
+        }
+      k += 8 * stride;
+      const bool more = k + 7 * stride < end;
+      uint2 n0[4], n1[4];
+      if (more) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          n0[u] = __ldg(cv + k + u * stride);
+          n1[u] = __ldg(cv + k + (u + 4) * stride);
+        }
+      }
+      mac_step<B, FE, L>(e0, g0, M, acc);
+      mac_step<B, FE, L>(e1, g1, M, acc);
+      if (!more) break;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        e0[u] = n0[u];
+        e1[u] = n1[u];
+      }
+    }
+  }
+  while (k < end) {  // at most two steps of four, the last one clamped
+    uint2 e[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const uint32_t kk = k + u * stride;
+      e[u] = __ldg(cv + (kk < end ? kk : k));
+      if (kk >= end) e[u].y = 0u;
+    }
+    uint4 g[4][NV];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) g[u][v] = __ldg(Xs + (size_t)e[u].x * RW + v * TPR);
+    mac_step<B, FE, L>(e, g, M, acc);
+    k += 4 * stride;
+  }
+}
+
 __device__ __forceinline__ int pair_index(int i, int j, int B) { return i * B - i * (i - 1) / 2 + (j - i); }
 
 // ---------------------------------------------------------------- Gram terms
@@ -1172,9 +1238,13 @@ __global__ void barrier_check_kernel(unsigned int* bar, int* error, uint64_t lim
 // within about one chunk's time of its last warp.  Lanes form RPW slots of TPR
 // threads; slot s takes entries beg+s, beg+s+RPW, ...  The slot sums (exact
 // residues) are combined with shuffles and added to heavy_acc with 64-bit
-// atomics.  (4 lanes per thread at widths 16 and 32, a whole gathered row per
-// load instruction, measured slower: fewer bytes in flight per thread.)
-template <int B, int FE, int L = kDefaultLpt<B>>
+// atomics.  At widths 16 and 32 a thread holds 4 lanes and sums eight entries
+// per step (gather_sum8): a whole gathered row per load instruction, as many
+// bytes in flight as 8 lanes and four entries.
+template <int B>
+constexpr int kChunkLpt = (B >= 16) ? 4 : kDefaultLpt<B>;
+
+template <int B, int FE, int L = kChunkLpt<B>>
 __global__ void __launch_bounds__(kThreads, 3) chunk_kernel(ChunkParams P) {
   using S = Shape<B, L>;
   constexpr int LPT = S::LPT, TPR = S::TPR, RPW = S::RPW;
@@ -1192,7 +1262,10 @@ __global__ void __launch_bounds__(kThreads, 3) chunk_kernel(ChunkParams P) {
     uint64_t acc[LPT];
 #pragma unroll
     for (int l = 0; l < LPT; ++l) acc[l] = 0;
-    gather_sum<B, FE, false, L>(P.cv, beg + slot, end, (uint32_t)RPW, P.X, sub, M, acc);
+    if constexpr (L == 4 && B >= 16)
+      gather_sum8<B, FE, L>(P.cv, beg + slot, end, (uint32_t)RPW, P.X, sub, M, acc);
+    else
+      gather_sum<B, FE, false, L>(P.cv, beg + slot, end, (uint32_t)RPW, P.X, sub, M, acc);
     uint32_t y[LPT];
 #pragma unroll
     for (int l = 0; l < LPT; ++l) y[l] = reduce(acc[l], M);
