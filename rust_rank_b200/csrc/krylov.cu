@@ -829,6 +829,17 @@ __device__ __forceinline__ void byte_transpose4(const uint32_t (&v)[4], uint32_t
   w[3] = __byte_perm(t2, t3, 0x7632);
 }
 
+// y * s * 2^-32 mod p without the final correction: a value in [0, 2p) < 2^32
+// congruent to the Montgomery product.  The Gram pass only needs the value
+// mod p (its limb products are exact for any 32-bit operand and its sums are
+// reduced mod p), so the comparison and subtraction are left out.
+__device__ __forceinline__ uint32_t redc_lazy(uint32_t y, uint32_t s, const ModP& M) {
+  uint32_t lo = 0, hi = 0;
+  mac_cc(y, s, lo, hi);
+  mac_cc(lo * M.pinv, M.p, lo, hi);  // lo becomes 0; y s + q p < 2 p 2^32
+  return hi;
+}
+
 // A bounded wait that also ends when another role of the CTA gave up.
 __device__ __forceinline__ bool mbar_wait_or(uint32_t addr, uint32_t parity, const volatile int* abort) {
   const uint64_t t0 = tc_ns();
@@ -1075,7 +1086,7 @@ __global__ void __launch_bounds__(TcShape<B>::THREADS, 1) gram_tc_kernel(PassPar
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
           const uint32_t yv = c4 == 0 ? y[q].x : c4 == 1 ? y[q].y : c4 == 2 ? y[q].z : y[q].w;
-          z[q] = redc((uint64_t)yv * sc[q], M);
+          z[q] = redc_lazy(yv, sc[q], M);
           u[q] = P.gram_sym ? z[q] : yv;
         }
         uint32_t wz[4], wu[4];
