@@ -167,6 +167,7 @@ int rr_ctx_destroy(rr_ctx* ctx) {
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   cudaStreamDestroy(ctx->stream);
+  rr::staging_destroy(ctx->staging);
   delete ctx;
   return RR_OK;
 }
@@ -277,8 +278,7 @@ int rr_krylov_create(rr_matrix* mat, int32_t b, const uint32_t* row_precond, con
     // + 4: the Gram pass copies row scales in 16-byte pieces
     RR_TRY(kr->drinv_r.alloc_async(m + 4, s));
     RR_TRY(kr->dcinv_r.alloc_async(n + 4, s));
-    RR_CUDA(cudaMemcpyAsync(rp.ptr, row_precond, m * 4, cudaMemcpyHostToDevice, s));
-    RR_CUDA(cudaMemcpyAsync(cp.ptr, col_precond, n * 4, cudaMemcpyHostToDevice, s));
+    RR_TRY(rr::upload_host(mat->ctx, {{rp.ptr, row_precond, (size_t)m * 4}, {cp.ptr, col_precond, (size_t)n * 4}}, s));
     RR_TRY(launch_precond(kr.get(), rp.ptr, cp.ptr, mat->d_rowperm.ptr));
   }  // the staging buffers are freed in stream order, after the kernel
   const int B = kr->B;
@@ -311,7 +311,7 @@ int rr_krylov_create(rr_matrix* mat, int32_t b, const uint32_t* row_precond, con
   {
     DevBuf<uint32_t> v;
     RR_TRY(v.alloc_async((size_t)b * n, s));
-    RR_CUDA(cudaMemcpyAsync(v.ptr, curv, (size_t)b * n * 4, cudaMemcpyHostToDevice, s));
+    RR_TRY(rr::upload_host(mat->ctx, {{v.ptr, curv, (size_t)b * n * 4}}, s));
     RR_TRY(launch_scatter_block(kr.get(), v.ptr, kr->X[1].ptr));
     kr->cur = 0;
     // S_0 is computed now into slot 0 and published by the first advance

@@ -322,11 +322,11 @@ int matrix_build_device(rr_ctx* ctx, int64_t m, int64_t n, const int64_t* rowptr
   RR_TRY(cdeg.alloc_async(n, s));
   RR_TRY(bad.alloc_async(3, s));
   RR_TRY(maxdeg.alloc_async(2, s));
-  RR_CUDA(cudaMemcpyAsync(d_rowptr.ptr, rowptr, (m + 1) * 8, cudaMemcpyHostToDevice, s));
-  if (nnz) {
-    RR_CUDA(cudaMemcpyAsync(d_col.ptr, col, nnz * 4, cudaMemcpyHostToDevice, s));
-    RR_CUDA(cudaMemcpyAsync(d_val.ptr, val, nnz * 4, cudaMemcpyHostToDevice, s));
-  }
+  RR_TRY(upload_host(ctx,
+                     {{d_rowptr.ptr, rowptr, (size_t)(m + 1) * 8},
+                      {d_col.ptr, col, (size_t)nnz * 4},
+                      {d_val.ptr, val, (size_t)nnz * 4}},
+                     s));
   RR_CUDA(cudaMemsetAsync(bad.ptr, 0xff, 3 * 8, s));
   RR_CUDA(cudaMemsetAsync(maxdeg.ptr, 0, 2 * 4, s));
   RR_CUDA(cudaMemsetAsync(cdeg.ptr, 0, n * 4, s));

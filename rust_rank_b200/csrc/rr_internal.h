@@ -123,7 +123,12 @@ struct DevBuf {
 
 }  // namespace rr
 
+namespace rr {
+struct Staging;  // pinned staging buffers of host-to-device copies (upload.cpp)
+}
+
 struct rr_ctx_s {
+  rr::Staging* staging = nullptr;  // created at the first staged copy
   int device = 0;
   cudaStream_t stream = nullptr;
   int num_sms = 0;
@@ -142,6 +147,18 @@ struct DevCsr {
   int64_t nchunks = 0;
   DevBuf<uint32_t> chunk_row, chunk_begin, chunk_end;
 };
+
+// Host arrays to copy to the device: pageable arrays of 4 MB and more go
+// through the context's pinned staging buffers, several host threads copying
+// pieces while earlier pieces are in flight; the rest straight to
+// cudaMemcpyAsync.  Returns when the host arrays may be reused.
+struct HostSegment {
+  void* dst;
+  const void* src;
+  size_t bytes;
+};
+int upload_host(rr_ctx* ctx, const std::vector<HostSegment>& segs, cudaStream_t s);
+void staging_destroy(Staging* st);
 
 constexpr int64_t kHeavyDegree = 32;   // rows longer than this are split
 constexpr int64_t kChunkNnz = 1024;    // nonzeros per chunk of a split row
