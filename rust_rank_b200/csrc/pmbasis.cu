@@ -982,8 +982,17 @@ constexpr int kElimColsPerWarp = 6;  // 8 x 6 = 48 >= n + m
 static_assert(kElimWarps * kElimColsPerWarp >= kMmaRows + kMmaCols, "elimination columns");
 static_assert(kElimWarps <= kLeafWarps, "elimination warps");
 
-// Named barrier of the elimination warps (the others wait at __syncthreads).
+// Named barriers of the elimination warps and of the update warps.
 __device__ __forceinline__ void elim_bar() { asm volatile("bar.sync 1, %0;" ::"n"(kElimWarps * 32) : "memory"); }
+__device__ __forceinline__ void upd_bar() {
+  asm volatile("bar.sync 2, %0;" ::"n"((kLeafWarps - kElimWarps) * 32) : "memory");
+}
+constexpr uint64_t kLeafWaitNs = 2000000000ull;  // 2 s of %globaltimer per hand-off wait
+__device__ __forceinline__ uint64_t leaf_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 __device__ __forceinline__ void leaf_mma_u8(int (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
   asm volatile(
@@ -999,7 +1008,7 @@ __host__ __device__ constexpr int leaf_plane_words(int n) { return 32 * 8 * ((n 
 
 // Shared-memory bytes of pm_leaves_mma_kernel.
 size_t leaves_mma_smem_bytes(int m, int n, int K) {
-  size_t words = (size_t)2 * K * leaf_plane_words(n) + 1024 + (size_t)m * (m + 1) + (size_t)m * n + 2 * (size_t)m;
+  size_t words = (size_t)2 * K * leaf_plane_words(n) + 2048 + (size_t)m * (m + 1) + (size_t)m * n + 2 * (size_t)m;
   size_t bytes = (words * 4 + 15) & ~(size_t)15;
   bytes += 2 * (size_t)m * 8 + (size_t)m * 4 + 64;
   return bytes;
@@ -1024,16 +1033,18 @@ __global__ void __launch_bounds__(kLeafThreads) pm_leaves_mma_kernel(LeafParams 
   const uint32_t p = M.p;
   uint32_t* Rc = reinterpret_cast<uint32_t*>(smem_raw);  // [K][PW] residual byte planes
   uint32_t* Rn = Rc + K * PW;
-  uint32_t* Tp = Rn + K * PW;                             // [4][32 rows][8 words] byte planes of T
-  uint32_t* Tq = Tp + 1024;                               // [m][TQS]: Tq[s][i] = T[i][s]
+  uint32_t* Tp = Rn + K * PW;                             // 2 x [4][32 rows][8 words] byte planes of T
+  uint32_t* Tq = Tp + 2048;                               // [m][TQS]: Tq[s][i] = T[i][s]
   uint32_t* R0 = Tq + m * TQS;                            // [m][n]: coefficient 0 of the residual
   uint32_t* sigma = R0 + m * n;                           // m
   uint32_t* sig_tmp = sigma + m;                          // m
-  const size_t w32 = (size_t)2 * K * PW + 1024 + (size_t)m * TQS + (size_t)m * n + 2 * (size_t)m;
+  const size_t w32 = (size_t)2 * K * PW + 2048 + (size_t)m * TQS + (size_t)m * n + 2 * (size_t)m;
   int64_t* sdelta = reinterpret_cast<int64_t*>(smem_raw + ((w32 * 4 + 15) & ~(size_t)15));
   int64_t* sdelta_tmp = sdelta + m;
   int* perm = reinterpret_cast<int*>(sdelta_tmp + m);
-  __shared__ unsigned long long s_mx;
+  __shared__ unsigned long long s_mx2[2];     // pivot-row masks of the last two leaves
+  __shared__ volatile int s_tready, s_c1, s_abort;
+  __shared__ int s_ok_e, s_ok_u;
   __shared__ uint32_t rpart[2 * kRpartSize];  // first n columns of A, all rows, double buffered
 
   const int tid = threadIdx.x, nt = blockDim.x;
@@ -1042,7 +1053,7 @@ __global__ void __launch_bounds__(kLeafThreads) pm_leaves_mma_kernel(LeafParams 
   const uint32_t Wt[3] = {M.c32, (uint32_t)((uint64_t)M.c32 * 256 % p), (uint32_t)((uint64_t)M.c32 * 65536 % p)};
 
   // padding bytes (rows i >= m of every column, columns c >= n) stay zero for good
-  for (int e = tid; e < 2 * K * PW + 1024; e += nt) Rc[e] = 0;
+  for (int e = tid; e < 2 * K * PW + 2048; e += nt) Rc[e] = 0;
   __syncthreads();
   for (int e = tid; e < K * m * n; e += nt) {
     const int t = e / (m * n), i = (e / n) % m, c = e % n;
@@ -1056,8 +1067,104 @@ __global__ void __launch_bounds__(kLeafThreads) pm_leaves_mma_kernel(LeafParams 
   }
   __syncthreads();
 
-  for (int leaf = 0; leaf < K; ++leaf) {
-    if (warp < kElimWarps) {
+  // Two warp groups overlap consecutive leaves: the elimination warps (E,
+  // warps 0 .. kElimWarps-1) run leaf k+1 while the update warps (U, the
+  // others) still apply T_k to the remaining coefficients of the residual.
+  // Leaf k+1 needs only coefficient 0 of the new residual, which E computes
+  // itself (from coefficients 0 and 1 of the old one); U computes the others,
+  // coefficient 1 first.  Residual buffer j & 1 holds the residual before leaf
+  // j; E writes only coefficient 0 of a buffer and U only coefficients >= 1,
+  // and T_k's byte planes and mask are double buffered by k & 1.  Hand-offs are
+  // counters in shared memory: s_tready = k + 1 once T_k, its mask and the new
+  // coefficient 0 are written (U may start on leaf k), s_c1 = k + 1 once U has
+  // written coefficient 1 of the residual after leaf k (E may take T_{k+1} and
+  // reuse T_{k-1}'s planes).  A wait gives up after kLeafWaitNs, raises
+  // s_abort and sets *P.status = 3; both groups then leave their loops.
+  if (tid == 0) {
+    s_tready = 0;
+    s_c1 = 0;
+    s_abort = 0;
+  }
+  __syncthreads();
+  const int tiles = MT * NT;  // 1, 2 or 4: a divisor of the group's warp count
+  auto wait_count = [&](volatile int* cnt, int target) -> bool {
+    const uint64_t t0 = leaf_ns();
+    while (*cnt < target) {
+      if (s_abort) return false;
+      if (leaf_ns() - t0 > kLeafWaitNs) {
+        s_abort = 1;
+        atomicExch(P.status, 3);
+        return false;
+      }
+      __nanosleep(32);
+    }
+    __threadfence_block();
+    return true;
+  };
+  // outputs t in [tmin, tmax] (and < rem) of Rn[t][i] = T_i . Rc[t + 1 - mask_i],
+  // from the products T Rc[tq] for the tq of this warp's share
+  auto residual = [&](int gw, int gwarps, int tq_first, int tq_last, int tmin, int tmax, const uint32_t* Tpl,
+                      const uint32_t* Rcl, uint32_t* Rnl, unsigned long long mx, int rem) {
+    const int tile = gw % tiles, tq0 = tq_first + gw / tiles, tqs = gwarps / tiles;
+    const int mt = tile / NT, ntl = tile % NT;
+    const int r0 = mt * 16 + g, r1 = r0 + 8, col = ntl * 8 + g;
+    if (tq0 > tq_last) return;
+    uint32_t A[4][4];
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+      A[l][0] = Tpl[l * 256 + plane_word(r0, t4)];
+      A[l][1] = Tpl[l * 256 + plane_word(r1, t4)];
+      A[l][2] = Tpl[l * 256 + plane_word(r0, t4 + 4)];
+      A[l][3] = Tpl[l * 256 + plane_word(r1, t4 + 4)];
+    }
+    for (int tq = tq0; tq <= tq_last; tq += tqs) {
+      uint32_t Bf[4][2];
+      const uint32_t* rc = Rcl + tq * PW;
+#pragma unroll
+      for (int l = 0; l < 4; ++l) {
+        Bf[l][0] = rc[l * NPc * 8 + plane_word(col, t4)];
+        Bf[l][1] = rc[l * NPc * 8 + plane_word(col, t4 + 4)];
+      }
+      int C[7][4];
+#pragma unroll
+      for (int s = 0; s < 7; ++s)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) C[s][v] = 0;
+#pragma unroll
+      for (int l = 0; l < 4; ++l)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) leaf_mma_u8(C[l + r], A[l], Bf[r][0], Bf[r][1]);
+      // classes 0..3 exactly in 64 bits (< 2^48), classes 4..6 with their weights
+      uint32_t lo[4], hi[4];
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const uint64_t x = (uint64_t)(uint32_t)C[0][v] + ((uint64_t)(uint32_t)C[1][v] << 8) +
+                           ((uint64_t)(uint32_t)C[2][v] << 16) + ((uint64_t)(uint32_t)C[3][v] << 24);
+        lo[v] = (uint32_t)x;
+        hi[v] = (uint32_t)(x >> 32);
+        mac_cc((uint32_t)C[4][v], Wt[0], lo[v], hi[v]);
+        mac_cc((uint32_t)C[5][v], Wt[1], lo[v], hi[v]);
+        mac_cc((uint32_t)C[6][v], Wt[2], lo[v], hi[v]);
+      }
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const int row = (v < 2) ? r0 : r1;
+        const int c = ntl * 8 + 2 * t4 + (v & 1);
+        if (row < m && c < n) {
+          const int t = tq - 1 + (int)((mx >> row) & 1ull);
+          if (t >= tmin && t <= tmax && t < rem) {
+            const uint32_t val = redc_cc(lo[v], hi[v], M);
+            plane_store(Rnl + t * PW, NPc, c, row, val);
+            if (t == 0) R0[row * n + c] = val;
+          }
+        }
+      }
+    }
+  };
+  uint32_t* const Rbuf[2] = {Rc, Rn};
+
+  if (warp < kElimWarps) {
+    for (int leaf = 0; leaf < K; ++leaf) {
       // stable sort of delta, descending (src/sigma_basis.rs:357-359): lane q
       // takes the row of sorted position q
       if (warp == 0 && lane < m) {
@@ -1071,7 +1178,7 @@ __global__ void __launch_bounds__(kLeafThreads) pm_leaves_mma_kernel(LeafParams 
       }
       elim_bar();
       const int myrow = lane < m ? perm[lane] : 0;
-      // this warp's 12 columns of row `lane` of A = [pi r | pi] (src/sigma_basis.rs:369-380)
+      // this warp's columns of row `lane` of A = [pi r | pi] (src/sigma_basis.rs:369-380)
       const int c0 = kElimColsPerWarp * warp;
       uint32_t a[kElimColsPerWarp];
 #pragma unroll
@@ -1146,7 +1253,7 @@ __global__ void __launch_bounds__(kLeafThreads) pm_leaves_mma_kernel(LeafParams 
         if (lane < m) sdelta_tmp[lane] = sdelta[myrow] - (piv_row ? 1 : 0);  // src/sigma_basis.rs:408-411
         if (lane == 0) {
           P.mask[leaf] = mx;
-          s_mx = mx;
+          s_mx2[leaf & 1] = mx;
         }
       }
       elim_bar();
@@ -1154,87 +1261,62 @@ __global__ void __launch_bounds__(kLeafThreads) pm_leaves_mma_kernel(LeafParams 
         sigma[lane] = sig_tmp[lane];
         sdelta[lane] = sdelta_tmp[lane];
       }
-    }
-    __syncthreads();
-    const int rem = K - leaf - 1;
-    if (rem == 0) break;
-    // byte planes of T: row i, word w holds limb l of T[i][4w .. 4w+3]
-    for (int e = tid; e < m * 8; e += nt) {
-      const int i = e >> 3, w = e & 7;
-      uint32_t v[4];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) v[j] = (4 * w + j < m) ? Tq[(4 * w + j) * TQS + i] : 0u;
-#pragma unroll
-      for (int l = 0; l < 4; ++l) {
-        const uint32_t lo = __byte_perm(v[0], v[1], 0x40 + 0x11 * l) & 0xffffu;  // byte l of v0, byte l of v1
-        const uint32_t hi = __byte_perm(v[2], v[3], 0x40 + 0x11 * l) & 0xffffu;
-        Tp[l * 256 + plane_word(i, w)] = lo | (hi << 16);
+      const int rem = K - leaf - 1;
+      if (rem == 0) break;
+      // coefficient 1 of this leaf's residual is U's (leaf - 1 > = 0), and
+      // U's work on leaf - 1 no longer reads the planes of T_{leaf - 2}
+      if (leaf > 0) {
+        if (tid == 0) s_ok_e = wait_count(&s_c1, leaf) ? 1 : 0;
+        elim_bar();
+        if (!s_ok_e) break;
       }
-    }
-    __syncthreads();
-    // residual: Rn[t][i] = T_i . Rc[t + 1 - mask_i] for t < rem, from the
-    // products P[t'] = T Rc[t'] (t' <= rem); tile (t', mt, nt) per warp
-    const unsigned long long mx = s_mx;
-    const int tiles = MT * NT;  // 1, 2 or 4: a divisor of the warp count
-    const int tile = warp % tiles, tq0 = warp / tiles, tqs = kLeafWarps / tiles;
-    const int mt = tile / NT, ntl = tile % NT;
-    const int r0 = mt * 16 + g, r1 = r0 + 8, col = ntl * 8 + g;
-    uint32_t A[4][4];
+      uint32_t* const Tpl = Tp + (leaf & 1) * 1024;
+      // byte planes of T: row i, word w holds limb l of T[i][4w .. 4w+3]
+      for (int e = tid; e < m * 8; e += kElimWarps * 32) {
+        const int i = e >> 3, w = e & 7;
+        uint32_t v[4];
 #pragma unroll
-    for (int l = 0; l < 4; ++l) {
-      A[l][0] = Tp[l * 256 + plane_word(r0, t4)];
-      A[l][1] = Tp[l * 256 + plane_word(r1, t4)];
-      A[l][2] = Tp[l * 256 + plane_word(r0, t4 + 4)];
-      A[l][3] = Tp[l * 256 + plane_word(r1, t4 + 4)];
-    }
-    for (int tq = tq0; tq <= rem; tq += tqs) {
-      uint32_t Bf[4][2];
-      const uint32_t* rc = Rc + tq * PW;
+        for (int j = 0; j < 4; ++j) v[j] = (4 * w + j < m) ? Tq[(4 * w + j) * TQS + i] : 0u;
 #pragma unroll
-      for (int l = 0; l < 4; ++l) {
-        Bf[l][0] = rc[l * NPc * 8 + plane_word(col, t4)];
-        Bf[l][1] = rc[l * NPc * 8 + plane_word(col, t4 + 4)];
-      }
-      int C[7][4];
-#pragma unroll
-      for (int s = 0; s < 7; ++s)
-#pragma unroll
-        for (int v = 0; v < 4; ++v) C[s][v] = 0;
-#pragma unroll
-      for (int l = 0; l < 4; ++l)
-#pragma unroll
-        for (int r = 0; r < 4; ++r) leaf_mma_u8(C[l + r], A[l], Bf[r][0], Bf[r][1]);
-      // classes 0..3 exactly in 64 bits (< 2^48), classes 4..6 with their weights
-      uint32_t lo[4], hi[4];
-#pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        const uint64_t x = (uint64_t)(uint32_t)C[0][v] + ((uint64_t)(uint32_t)C[1][v] << 8) +
-                           ((uint64_t)(uint32_t)C[2][v] << 16) + ((uint64_t)(uint32_t)C[3][v] << 24);
-        lo[v] = (uint32_t)x;
-        hi[v] = (uint32_t)(x >> 32);
-        mac_cc((uint32_t)C[4][v], Wt[0], lo[v], hi[v]);
-        mac_cc((uint32_t)C[5][v], Wt[1], lo[v], hi[v]);
-        mac_cc((uint32_t)C[6][v], Wt[2], lo[v], hi[v]);
-      }
-#pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        const int row = (v < 2) ? r0 : r1;
-        const int c = ntl * 8 + 2 * t4 + (v & 1);
-        if (row < m && c < n) {
-          const int t = tq - 1 + (int)((mx >> row) & 1ull);
-          if (t >= 0 && t < rem) {
-            const uint32_t val = redc_cc(lo[v], hi[v], M);
-            plane_store(Rn + t * PW, NPc, c, row, val);
-            if (t == 0) R0[row * n + c] = val;
-          }
+        for (int l = 0; l < 4; ++l) {
+          const uint32_t lo = __byte_perm(v[0], v[1], 0x40 + 0x11 * l) & 0xffffu;  // byte l of v0, byte l of v1
+          const uint32_t hi = __byte_perm(v[2], v[3], 0x40 + 0x11 * l) & 0xffffu;
+          Tpl[l * 256 + plane_word(i, w)] = lo | (hi << 16);
         }
       }
+      elim_bar();
+      // coefficient 0 of the next residual (products with coefficients 0 and 1)
+      residual(warp, kElimWarps, 0, std::min(1, rem), 0, 0, Tpl, Rbuf[leaf & 1], Rbuf[(leaf + 1) & 1],
+               s_mx2[leaf & 1], rem);
+      elim_bar();
+      if (tid == 0) {
+        __threadfence_block();
+        s_tready = leaf + 1;
+      }
     }
-    __syncthreads();
-    uint32_t* tr = Rc;
-    Rc = Rn;
-    Rn = tr;
+  } else {
+    const int uw = warp - kElimWarps, uwarps = kLeafWarps - kElimWarps;
+    for (int leaf = 0; leaf + 1 < K; ++leaf) {
+      if (tid == kElimWarps * 32) s_ok_u = wait_count(&s_tready, leaf + 1) ? 1 : 0;
+      upd_bar();
+      if (!s_ok_u) break;
+      const int rem = K - leaf - 1;
+      const uint32_t* Tpl = Tp + (leaf & 1) * 1024;
+      const uint32_t* Rcl = Rbuf[leaf & 1];
+      uint32_t* Rnl = Rbuf[(leaf + 1) & 1];
+      const unsigned long long mx = s_mx2[leaf & 1];
+      // coefficient 1 first (products with coefficients 1 and 2), then the rest
+      residual(uw, uwarps, 1, std::min(2, rem), 1, rem - 1, Tpl, Rcl, Rnl, mx, rem);
+      upd_bar();
+      if (tid == kElimWarps * 32) {
+        __threadfence_block();
+        s_c1 = leaf + 1;
+      }
+      residual(uw, uwarps, 3, rem, 1, rem - 1, Tpl, Rcl, Rnl, mx, rem);
+      upd_bar();
+    }
   }
+  __syncthreads();
   for (int i = tid; i < m; i += nt) {
     P.sigma_inv[i] = inv_fermat(sigma[i], M);
     P.delta[i] = sdelta[i];
@@ -1909,6 +1991,7 @@ int pm_basis_batch_device(rr_ctx* ctx, int nb, const uint32_t* const* seqs, cons
   }
   RR_CUDA(cudaMemcpyAsync(&status, P.status.ptr, sizeof(int), cudaMemcpyDeviceToHost, P.s));
   RR_CUDA(cudaStreamSynchronize(P.s));
+  if (status == 3) return fail(RR_ETIMEOUT, "PM-basis leaf kernel: a hand-off between its warp groups gave up");
   if (status) return fail(RR_ECUDA, "PM-basis device status %d (zero row scale)", status);
   return RR_OK;
 }
