@@ -547,8 +547,7 @@ int rr_batch_create(rr_ctx* ctx, int32_t nmat, const int64_t* m, const int64_t* 
   cudaStream_t st = ctx->stream;
   auto up = [&](auto& buf, const auto& vec) -> int {
     RR_TRY(buf.alloc(std::max<size_t>(vec.size(), 1)));
-    if (!vec.empty())
-      RR_CUDA(cudaMemcpyAsync(buf.ptr, vec.data(), vec.size() * sizeof(vec[0]), cudaMemcpyHostToDevice, st));
+    if (!vec.empty()) RR_TRY(upload_host(ctx, {{buf.ptr, vec.data(), vec.size() * sizeof(vec[0])}}, st));
     return RR_OK;
   };
   bt->A.rows = Mtot;
