@@ -138,10 +138,10 @@ __global__ void pack_kernel(const uint64_t* __restrict__ key, const uint32_t* __
 }
 
 // count[0] += rows of degree > kHeavyDegree.
-__global__ void heavy_count_kernel(const uint32_t* __restrict__ deg, int64_t n, unsigned int* count) {
+__global__ void count_above_kernel(const uint32_t* __restrict__ deg, int64_t n, uint32_t above, unsigned int* count) {
   unsigned int c = 0;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    c += deg[i] > (uint32_t)kHeavyDegree;
+    c += deg[i] > above;
   for (int off = 16; off > 0; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
   if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
 }
@@ -291,16 +291,18 @@ int build_chunks(DevCsr& d, int64_t heavy, cudaStream_t s) {
   return RR_OK;
 }
 
-int heavy_rows_of(const uint32_t* deg, int64_t n, cudaStream_t s, int64_t* heavy) {
+// Rows of degree above `above` (rows are in decreasing degree order, so these
+// are the first ones).
+int rows_above(const uint32_t* deg, int64_t n, uint32_t above, cudaStream_t s, int64_t* count) {
   DevBuf<unsigned int> cnt;
   RR_TRY(cnt.alloc_async(1, s));
   RR_CUDA(cudaMemsetAsync(cnt.ptr, 0, 4, s));
-  heavy_count_kernel<<<build_grid(n), kBuildThreads, 0, s>>>(deg, n, cnt.ptr);
+  count_above_kernel<<<build_grid(n), kBuildThreads, 0, s>>>(deg, n, above, cnt.ptr);
   RR_CUDA(cudaGetLastError());
   unsigned int h = 0;
   RR_CUDA(cudaMemcpyAsync(&h, cnt.ptr, 4, cudaMemcpyDeviceToHost, s));
   RR_CUDA(cudaStreamSynchronize(s));
-  *heavy = h;
+  *count = h;
   return RR_OK;
 }
 
@@ -390,8 +392,10 @@ int matrix_build_device(rr_ctx* ctx, int64_t m, int64_t n, const int64_t* rowptr
     RR_CUDA(cudaGetLastError());
   }
   int64_t heavyA = 0, heavyT = 0;
-  RR_TRY(heavy_rows_of(rdeg_new.ptr, m, s, &heavyA));
-  RR_TRY(heavy_rows_of(cdeg_new.ptr, n, s, &heavyT));
+  RR_TRY(rows_above(rdeg_new.ptr, m, (uint32_t)kHeavyDegree, s, &heavyA));
+  RR_TRY(rows_above(cdeg_new.ptr, n, (uint32_t)kHeavyDegree, s, &heavyT));
+  RR_TRY(rows_above(rdeg_new.ptr, m, 0u, s, &A.live_rows));
+  RR_TRY(rows_above(cdeg_new.ptr, n, 0u, s, &At.live_rows));
   RR_TRY(build_chunks(A, heavyA, s));
   RR_TRY(build_chunks(At, heavyT, s));
   RR_CUDA(cudaStreamSynchronize(s));

@@ -535,6 +535,14 @@ __device__ __forceinline__ void pass_body(const PassParams& P, uint32_t* gram_sm
       }
     }
     const int64_t r = batch * RPW + slot;
+    if (P.tail_begin > 0 && batch * RPW >= P.tail_begin) {
+      // a batch of rows without entries: zero output, nothing to the Gram term
+      if (r < P.rows) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) P.Y[r * (B / 4) + S::word_of(sub, v)] = make_uint4(0, 0, 0, 0);
+      }
+      continue;
+    }
     uint32_t gz[LPT], gu[LPT];
     if (r < P.rows) {
       uint32_t t[LPT];
@@ -1696,6 +1704,7 @@ int krylov_launch_application(rr_krylov* kr, cudaEvent_t* ev) {
   P.cv = mat->A.cv.ptr;
   P.rows = mat->A.rows;
   P.heavy_rows = mat->A.heavy_rows;
+  P.tail_begin = mat->A.live_rows;
   P.X = reinterpret_cast<const uint4*>(x);
   P.Y = reinterpret_cast<uint4*>(kr->U.ptr);
   P.scale = kr->dr_m.ptr;
@@ -1710,7 +1719,7 @@ int krylov_launch_application(rr_krylov* kr, cudaEvent_t* ev) {
   // odd term: sum over rows of z (x) U with z = U d_r^{-1}
   if (!fused_odd) {
     PassParams G = base_params(kr);
-    G.rows = mat->A.rows;
+    G.rows = mat->A.live_rows > 0 ? mat->A.live_rows : mat->A.rows;  // zero rows add nothing
     G.X = reinterpret_cast<const uint4*>(kr->U.ptr);
     G.scale = kr->drinv_r.ptr;
     G.gram_sym = 0;
@@ -1726,6 +1735,7 @@ int krylov_launch_application(rr_krylov* kr, cudaEvent_t* ev) {
   P.cv = mat->At.cv.ptr;
   P.rows = mat->At.rows;
   P.heavy_rows = mat->At.heavy_rows;
+  P.tail_begin = mat->At.live_rows;
   P.X = reinterpret_cast<const uint4*>(kr->U.ptr);
   P.Y = reinterpret_cast<uint4*>(xn);
   P.scale = kr->dc_m.ptr;
@@ -1739,7 +1749,7 @@ int krylov_launch_application(rr_krylov* kr, cudaEvent_t* ev) {
   // even term: sum over rows of w' (x) w' with w' = x' d_c^{-1}
   if (!fused_even) {
     PassParams G = base_params(kr);
-    G.rows = mat->At.rows;
+    G.rows = mat->At.live_rows > 0 ? mat->At.live_rows : mat->At.rows;  // zero rows add nothing
     G.X = reinterpret_cast<const uint4*>(xn);
     G.scale = kr->dcinv_r.ptr;
     G.gram_sym = 1;

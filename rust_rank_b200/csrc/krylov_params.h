@@ -15,6 +15,9 @@ struct PassParams {
   const uint2* cv;          // packed (column, value)
   int64_t rows;
   int64_t heavy_rows;
+  // rows >= tail_begin have no entries (the end of the degree order): their
+  // output rows are zero and they add nothing to the Gram term (0 = no tail)
+  int64_t tail_begin;
   const uint4* X;           // gathered block [cols][B/4]   (kModeInit: w [rows][B/4])
   uint4* Y;                 // output block   [rows][B/4]
   const uint32_t* scale;    // odd: d_r R^2; even: d_c R^2; init: d_c R   (all mod p)

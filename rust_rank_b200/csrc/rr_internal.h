@@ -144,6 +144,7 @@ struct DevCsr {
   DevBuf<uint2> cv;         // packed (column, value) per entry
   int64_t rows = 0, cols = 0, nnz = 0;
   int64_t heavy_rows = 0;
+  int64_t live_rows = 0;    // rows with at least one entry: rows [0, live_rows)
   int64_t nchunks = 0;
   DevBuf<uint32_t> chunk_row, chunk_begin, chunk_end;
 };
