@@ -295,7 +295,8 @@ int rr_krylov_create(rr_matrix* mat, int32_t b, const uint32_t* row_precond, con
   RR_TRY(kr->counter.alloc_async(4, s));
   RR_CUDA(cudaMemsetAsync(kr->counter.ptr, 0, kr->counter.bytes(), s));
   RR_TRY(kr->d_term.alloc_async(1, s));
-  RR_TRY(kr->chunk_next.alloc_async(1, s));
+  RR_TRY(kr->chunk_next.alloc_async(2, s));
+  RR_CUDA(cudaMemsetAsync(kr->chunk_next.ptr, 0, 2 * sizeof(unsigned int), s));
   RR_TRY(kr->d_sptr.alloc_async(1, s));
   {
     // first application's odd term: slot 1 after S_0 of a fresh start, slot 0 on resume

@@ -231,6 +231,15 @@ __device__ __forceinline__ void gather_sum8(const uint2* __restrict__ cv, uint32
 
 __device__ __forceinline__ int pair_index(int i, int j, int B) { return i * B - i * (i - 1) / 2 + (j - i); }
 
+// Programmatic dependent launch: the single-matrix kernels are launched so
+// that the next kernel of an application may be scheduled while the previous
+// one finishes.  griddep_wait() blocks until the previous kernel has completed
+// and its writes are visible (it returns at once for a normal launch), so every
+// such kernel calls it before reading what its predecessor wrote;
+// griddep_launch() tells the scheduler a CTA has no more main-loop work.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // ---------------------------------------------------------------- Gram terms
 // Both accumulators sum G[i][j] = sum over rows of gz[i] * gu[j] (i <= j) for
 // the rows a warp processes, then add their residues into the CTA's red[].
@@ -606,6 +615,7 @@ __device__ __forceinline__ void pass_body(const PassParams& P, uint32_t* gram_sm
     }
     if (emit) gram.add(gz, gu, slot, sub, lane, M, W);
   }
+  if (!segmented) griddep_launch();
 
   if (!emit) return;
   gram.finish(slot, sub, lane, M, W);
@@ -691,6 +701,7 @@ __global__ void __launch_bounds__(kThreads, (B >= 32 && GRAM ? 2 : 4)) pass_kern
   extern __shared__ __align__(16) uint32_t gram_smem[];
   __shared__ unsigned long long red[B * (B + 1) / 2];
   __shared__ bool is_last;
+  griddep_wait();
   pass_body<B, MODE, FE, false, GRAM, L>(P, gram_smem, red, is_last);
 }
 
@@ -946,6 +957,7 @@ __global__ void __launch_bounds__(TcShape<B>::THREADS, 1) gram_tc_kernel(PassPar
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_base_s;
+  griddep_wait();  // the block this pass reads was written by the previous kernel
 
   const int64_t ntiles = (P.rows + T::TILE - 1) / T::TILE;
   const int64_t mine = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;  // tiles of this CTA
@@ -1114,6 +1126,7 @@ __global__ void __launch_bounds__(TcShape<B>::THREADS, 1) gram_tc_kernel(PassPar
       }
     }
   }
+  griddep_launch();
   __syncthreads();
   if (s_fail) {  // let what was committed or fetched finish before the memory goes away
     if (tid == 32) {
@@ -1271,11 +1284,20 @@ __global__ void __launch_bounds__(kThreads, 3) chunk_kernel(ChunkParams P) {
   const int sub = lane % TPR;
   const int slot = lane / TPR;
   const ModP M = P.M;
+  griddep_wait();
   for (;;) {
     unsigned int ticket = 0;
     if (lane == 0) ticket = atomicAdd(P.next, 1u);
     const int64_t ch = __shfl_sync(0xffffffffu, ticket, 0);
-    if (ch >= P.nchunks) break;
+    if (ch >= P.nchunks) {
+      // the last warp of the launch to run out of chunks (all tickets are
+      // taken by then) rewinds the dispenser for the next launch
+      if (lane == 0 && atomicAdd(P.next + 1, 1u) == gridDim.x * (unsigned)kWarps - 1u) {
+        P.next[0] = 0u;
+        P.next[1] = 0u;
+      }
+      break;
+    }
     const uint32_t beg = P.chunk_begin[ch], end = P.chunk_end[ch];
     const uint32_t row = P.chunk_row[ch];
     uint64_t acc[LPT];
@@ -1299,6 +1321,7 @@ __global__ void __launch_bounds__(kThreads, 3) chunk_kernel(ChunkParams P) {
       for (int l = 0; l < LPT; ++l) atomicAdd(&h[S::lane_of(sub, l)], (unsigned long long)y[l]);
     }
   }
+  griddep_launch();
 }
 
 // x[c'][l] = (l < b) ? V[l][colperm[c']] : 0   (V vector-major, original order)
@@ -1390,6 +1413,13 @@ static int launch_ex(const rr_krylov* kr, void (*fn)(Args...), dim3 grid, dim3 b
   cfg.blockDim = block;
   cfg.dynamicSmemBytes = smem;
   cfg.stream = s;
+  // the kernel may be scheduled while its predecessor on the stream finishes;
+  // it waits for it (griddep_wait) before reading the predecessor's output
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
   (void)kr;
   RR_CUDA(cudaLaunchKernelEx(&cfg, fn, args...));
   return RR_OK;
@@ -1682,10 +1712,8 @@ static int run_chunks(rr_krylov* kr, const DevCsr& A, const uint32_t* X) {
   C.nchunks = A.nchunks;
   C.X = reinterpret_cast<const uint4*>(X);
   C.heavy_acc = kr->heavy_acc.ptr;
-  C.next = kr->chunk_next.ptr;
+  C.next = kr->chunk_next.ptr;  // [ticket, warps done], zero between launches
   C.M = kr->M;
-  cudaStream_t s = kr->launch_stream ? kr->launch_stream : kr->mat->ctx->stream;
-  RR_CUDA(cudaMemsetAsync(kr->chunk_next.ptr, 0, sizeof(unsigned int), s));
   return launch_chunk(kr, C);
 }
 

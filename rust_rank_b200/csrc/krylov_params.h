@@ -65,7 +65,7 @@ struct ChunkParams {
   int64_t nchunks;
   const uint4* X;
   unsigned long long* heavy_acc;
-  unsigned int* next;  // chunk dispenser: zero at launch, one ticket per warp fetch
+  unsigned int* next;  // chunk dispenser [next ticket, warps done]: zero at launch, rewound by the last warp
   ModP M;
 };
 
