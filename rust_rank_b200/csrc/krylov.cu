@@ -696,8 +696,15 @@ __device__ __forceinline__ void pass_body(const PassParams& P, uint32_t* gram_sm
 // worth a few spilled registers (measured on the 2M x 1.5M Zipf matrix).  At
 // B = 32 the Gram accumulators alone take 48 registers, and two CTAs per SM
 // with 128 registers run the same matrix 1.2x faster than four with spills.
+//
+// Resident CTAs per SM the register budget is set for: 5 for the lean pass at
+// width 16 (48 registers; one more CTA of latency hiding measured 1.3 % faster
+// than 4 with 62 registers), 2 for fused passes at width 32, else 4.
+template <int B, bool GRAM>
+constexpr int kPassMinBlocks = (B >= 32 && GRAM) ? 2 : ((!GRAM && B == 16) ? 5 : 4);
+
 template <int B, int MODE, int FE, bool GRAM = true, int L = kDefaultLpt<B>>
-__global__ void __launch_bounds__(kThreads, (B >= 32 && GRAM ? 2 : 4)) pass_kernel(PassParams P) {
+__global__ void __launch_bounds__(kThreads, kPassMinBlocks<B, GRAM>) pass_kernel(PassParams P) {
   extern __shared__ __align__(16) uint32_t gram_smem[];
   __shared__ unsigned long long red[B * (B + 1) / 2];
   __shared__ bool is_last;
