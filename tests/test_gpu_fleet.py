@@ -77,29 +77,32 @@ def test_device_build_rejects_bad_input(ctx):
     assert e.value.status == 1 and "row 40" in str(e.value)
 
 
-def test_device_build_duplicates_empty_and_dense(ctx):
-    """Duplicate entries in a row, empty rows and columns, a dense row and a
-    dense column (chunked on both sides): same sequence as the oracle."""
+@pytest.mark.parametrize("b", [8, 16, 32])
+def test_device_build_duplicates_empty_and_dense(ctx, b):
+    """Duplicate entries in a row, empty rows and columns (the zero tail of
+    both degree orders), a dense row and a dense column (chunked on both
+    sides), at the widths of the fused, split and tcgen05 Gram forms: same
+    sequence and block as the oracle."""
     rng = np.random.default_rng(9)
     m, n = 2100, 1700
     rows = []
     for r in range(m):
         if r == 17:
-            c = np.arange(n)
+            c = np.arange(n - 60)  # the last 60 columns stay empty
         elif r % 11 == 0:
             c = np.array([], np.int64)
         else:
-            c = np.concatenate([rng.choice(n - 5, size=4), [3, 3, 999]])  # duplicates of column 3
+            c = np.concatenate([rng.choice(n - 100, size=4), [3, 3, 999]])  # duplicates of column 3
         rows.append(np.sort(c))
     rowptr = np.zeros(m + 1, np.int64)
     rowptr[1:] = np.cumsum([len(c) for c in rows])
     col = np.concatenate(rows).astype(np.int32)
     val = rng.integers(0, P, size=col.size).astype(np.uint32)
-    b = 8
     dr, dc = synth.preconditioners(m, n, P, 1)
     V = synth.random_vectors(b, n, P, 2)
     dm = rr.CsrMatrix.from_arrays(rowptr, col, val, m, n).to_device(P, ctx)
-    assert dm.max_nnzs() == (n, int(np.bincount(col, minlength=n).max()))
+    assert dm.max_nnzs() == (int(np.diff(rowptr).max()), int(np.bincount(col, minlength=n).max()))
+    assert int((np.bincount(col, minlength=n) == 0).sum()) == 60
     ks = rr.KrylovStream(dm, V, dr, dc, 0)
     seq = np.zeros((b * (b + 1) // 2, 20), np.uint32)
     L = ks.advance(16, seq)
